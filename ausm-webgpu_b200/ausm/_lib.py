@@ -1,0 +1,107 @@
+"""ctypes binding of libausm.so (include/ausm.h).
+
+The library is built in-tree by ausm-webgpu_b200/build.py.  There is no fallback: if
+the shared library is missing, importing the solver raises, so a GPU run can never
+silently take another path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import re
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parents[1]
+ROOT = PKG.parent
+LIB_PATH = Path(os.environ.get("AUSM_LIB", PKG / "lib" / "libausm.so"))
+HEADER = ROOT / "include" / "ausm.h"
+
+OK = 0
+ERR_INVALID, ERR_CUDA, ERR_OOM, ERR_DIVERGED, ERR_STATE, ERR_BUDGET, ERR_TIMEOUT, ERR_NOT_FOUND = range(-1, -9, -1)
+SCHEMES = {"SLAU2": 0, "SLAU": 1, "AUSM+-up": 2}
+ENGINES = {"fused": 0, "reference": 1}
+INIT = {"rest": 0, "freestream": 1}
+OUTER = {"rect": 0, "circle": 1}
+GRID = {"jacobi": 0, "multicolor": 1}
+FIELDS = {"density": 0, "pressure": 1, "temperature": 2, "mach": 3, "entropy": 4, "wave_speed": 5}
+
+
+class AusmError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"[{code}] {msg}")
+        self.code = code
+
+
+class AusmParams(C.Structure):
+    _fields_ = [("gamma", C.c_double), ("in_rho", C.c_double), ("in_pressure", C.c_double),
+                ("mach", C.c_double), ("aoa_deg", C.c_double), ("K_p", C.c_double), ("K_u", C.c_double),
+                ("cfl", C.c_double), ("maxdt", C.c_double), ("muscl", C.c_int), ("scheme", C.c_int),
+                ("ramp", C.c_double)]
+
+
+_lib = None
+
+_P = C.c_void_p
+_SIGS = {
+    "ausm_default_params": [C.POINTER(AusmParams)],
+    "ausm_set_device": [C.c_int],
+    "ausm_device_count": [C.POINTER(C.c_int)],
+    "ausm_create": [C.c_int, C.c_int, C.POINTER(C.c_void_p)],
+    "ausm_destroy": [_P],
+    "ausm_dims": [_P, C.POINTER(C.c_int), C.POINTER(C.c_int)],
+    "ausm_set_engine": [_P, C.c_int],
+    "ausm_set_params": [_P, C.POINTER(AusmParams)],
+    "ausm_get_params": [_P, C.POINTER(AusmParams)],
+    "ausm_set_scheme": [_P, C.c_int],
+    "ausm_set_body_naca4": [_P, C.c_int, C.c_double, C.c_double, C.c_int],
+    "ausm_naca4_points": [C.c_int, C.c_int, C.c_double, C.c_double, C.c_int, C.POINTER(C.c_double)],
+    "ausm_outer_points": [C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.POINTER(C.c_double)],
+    "ausm_set_body_points": [_P, C.POINTER(C.c_double), C.c_int],
+    "ausm_set_outer": [_P, C.c_int, C.c_double, C.c_double, C.c_double],
+    "ausm_set_radial_stretch": [_P, C.c_double],
+    "ausm_generate_grid": [_P, C.c_int, C.c_int, C.c_double, C.POINTER(C.c_int)],
+    "ausm_set_vertices": [_P, C.POINTER(C.c_float)],
+    "ausm_get_vertices": [_P, C.POINTER(C.c_float)],
+    "ausm_init_state": [_P, C.c_int],
+    "ausm_set_state": [_P, C.POINTER(C.c_float)],
+    "ausm_get_state": [_P, C.POINTER(C.c_float)],
+    "ausm_step": [_P, C.c_int, C.POINTER(C.c_float)],
+    "ausm_max_wave_speed": [_P, C.POINTER(C.c_float)],
+    "ausm_forces": [_P, C.POINTER(C.c_double), C.POINTER(C.c_double)],
+    "ausm_residual_l2": [_P, C.POINTER(C.c_double)],
+    "ausm_field": [_P, C.c_int, C.POINTER(C.c_float)],
+    "ausm_stream": [_P, C.POINTER(C.c_void_p)],
+    "ausm_synchronize": [_P],
+    "ausm_time_steps": [_P, C.c_int, C.c_int, C.POINTER(C.c_float)],
+}
+
+
+def header_functions() -> list[str]:
+    """Names of every function declared in include/ausm.h."""
+    txt = re.sub(r"/\*.*?\*/", "", HEADER.read_text(), flags=re.S)
+    return sorted(set(re.findall(r"^\s*(?:int|const char\*|void)\s+(ausm_\w+)\s*\(", txt, flags=re.M)))
+
+
+def lib():
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise AusmError(ERR_CUDA, f"{LIB_PATH} is not built: run python ausm-webgpu_b200/build.py")
+    L = C.CDLL(str(LIB_PATH))
+    for name, args in _SIGS.items():
+        if hasattr(L, name):
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = C.c_int
+    L.ausm_last_error.argtypes = [_P]
+    L.ausm_last_error.restype = C.c_char_p
+    _lib = L
+    return L
+
+
+def check(rc: int, handle=None):
+    if rc != OK:
+        msg = lib().ausm_last_error(handle)
+        raise AusmError(rc, msg.decode() if msg else "")
+    return rc

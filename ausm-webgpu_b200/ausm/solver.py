@@ -1,0 +1,203 @@
+"""Python host of libausm with the reference's operator surface.
+
+Names follow the reference's hooks (src/main.js, src/util.js, src/grid.js):
+  prepare_grid()     prepareGrid        main.js:658-707 (grid, then prepareState at rest)
+  prepare_state()    prepareState       main.js:631-655
+  update_solver()    updateSolver       main.js:629     ("SLAU2" | "SLAU" | "AUSM+-up")
+  set_params()       uni.values.*.set   util.js:162-190
+  step(n)            one frame of n RK3 steps with dt held fixed, main.js:744-791
+  forces()           forceCalc + forceIntegration, main.js:808-810
+Every call goes through the C ABI of libausm.so; errors raise AusmError with the
+library's message.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from ._lib import AusmError, AusmParams, check, lib
+
+
+def _fp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+def _dp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def set_device(device: int):
+    """Device for the solvers this thread creates next."""
+    check(lib().ausm_set_device(int(device)))
+
+
+def device_count() -> int:
+    n = C.c_int()
+    rc = lib().ausm_device_count(C.byref(n))
+    return n.value if rc == 0 else 0
+
+
+def default_params() -> AusmParams:
+    p = AusmParams()
+    check(lib().ausm_default_params(C.byref(p)))
+    return p
+
+
+class Solver:
+    """One O-grid solve of M (around the body) x N (radial) cells on the current GPU."""
+
+    def __init__(self, M: int, N: int, engine: str = "fused"):
+        self.M, self.N = int(M), int(N)
+        h = C.c_void_p()
+        check(lib().ausm_create(self.M, self.N, C.byref(h)))
+        self.h = h
+        if engine != "fused":
+            self.set_engine(engine)
+
+    # -- lifetime --
+    def close(self):
+        if getattr(self, "h", None):
+            lib().ausm_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _c(self, rc):
+        return check(rc, self.h)
+
+    # -- configuration --
+    def set_engine(self, engine: str):
+        self._c(lib().ausm_set_engine(self.h, _lib.ENGINES[engine]))
+
+    @property
+    def params(self) -> AusmParams:
+        p = AusmParams()
+        self._c(lib().ausm_get_params(self.h, C.byref(p)))
+        return p
+
+    def set_params(self, **kw):
+        """Update any AusmParams field: gamma, in_rho, in_pressure, mach, aoa_deg, K_p, K_u,
+        cfl, maxdt, muscl, scheme (name or index), ramp."""
+        p = self.params
+        for k, v in kw.items():
+            if k == "scheme" and isinstance(v, str):
+                v = _lib.SCHEMES[v]
+            if not hasattr(p, k):
+                raise AusmError(_lib.ERR_INVALID, f"unknown parameter {k}")
+            setattr(p, k, v)
+        self._c(lib().ausm_set_params(self.h, C.byref(p)))
+
+    def update_solver(self, name: str):
+        self._c(lib().ausm_set_scheme(self.h, _lib.SCHEMES[name]))
+
+    # -- geometry --
+    def set_body_naca4(self, digits: int, size: float = 0.3, x_offset: float = -0.7, closed_te: bool = True):
+        self._c(lib().ausm_set_body_naca4(self.h, int(digits), float(size), float(x_offset), int(closed_te)))
+
+    def set_body_points(self, xy):
+        a = np.ascontiguousarray(xy, dtype=np.float64).reshape(-1, 2)
+        self._c(lib().ausm_set_body_points(self.h, _dp(a), a.shape[0]))
+
+    def set_body_dat(self, text: str, size: float = 0.3, x_offset: float = -0.7):
+        from .geometry import sample_airfoil
+        self.set_body_points(sample_airfoil(text, self.M, size, x_offset))
+
+    def set_outer_rect(self, ratio: float = 1.5):
+        self._c(lib().ausm_set_outer(self.h, 0, float(ratio), 0.0, 0.0))
+
+    def set_outer_circle(self, radius: float, center=(0.0, 0.0)):
+        self._c(lib().ausm_set_outer(self.h, 1, float(radius), float(center[0]), float(center[1])))
+
+    def set_radial_stretch(self, first_spacing: float):
+        self._c(lib().ausm_set_radial_stretch(self.h, float(first_spacing)))
+
+    def generate_grid(self, iters: int = 10000, method: str = "jacobi", tol: float = 0.0) -> int:
+        done = C.c_int()
+        self._c(lib().ausm_generate_grid(self.h, int(iters), _lib.GRID[method], float(tol), C.byref(done)))
+        return done.value
+
+    def prepare_grid(self, iters: int = 10000, method: str = "jacobi", tol: float = 0.0) -> int:
+        """prepareGrid: generate the grid and restart the state at rest, as main.js:706 does."""
+        done = self.generate_grid(iters, method, tol)
+        self.prepare_state("rest")
+        return done
+
+    def set_vertices(self, xy):
+        a = np.ascontiguousarray(xy, dtype=np.float32).reshape(self.N + 1, self.M, 2)
+        self._c(lib().ausm_set_vertices(self.h, _fp(a)))
+
+    def vertices(self) -> np.ndarray:
+        a = np.zeros((self.N + 1, self.M, 2), dtype=np.float32)
+        self._c(lib().ausm_get_vertices(self.h, _fp(a)))
+        return a
+
+    # -- state --
+    def prepare_state(self, mode: str = "rest"):
+        self._c(lib().ausm_init_state(self.h, _lib.INIT[mode]))
+
+    def set_state(self, q):
+        a = np.ascontiguousarray(q, dtype=np.float32).reshape(self.N + 3, self.M, 4)
+        self._c(lib().ausm_set_state(self.h, _fp(a)))
+
+    def state(self, out: np.ndarray | None = None) -> np.ndarray:
+        """State in the reference layout; `out` (float32, contiguous, e.g. pinned) is
+        filled in place when given."""
+        a = np.zeros((self.N + 3, self.M, 4), dtype=np.float32) if out is None else out
+        if a.dtype != np.float32 or not a.flags.c_contiguous or a.size != (self.N + 3) * self.M * 4:
+            raise AusmError(_lib.ERR_INVALID, "out must be a contiguous float32 array of (N+3)*M*4 values")
+        self._c(lib().ausm_get_state(self.h, _fp(a)))
+        return a
+
+    def step(self, n: int = 1, wait: bool = True) -> float | None:
+        """n RK3 steps with dt fixed from the current state; returns that dt (f32)."""
+        if not wait:
+            self._c(lib().ausm_step(self.h, int(n), None))
+            return None
+        dt = C.c_float()
+        self._c(lib().ausm_step(self.h, int(n), C.byref(dt)))
+        return dt.value
+
+    def max_wave_speed(self) -> float:
+        w = C.c_float()
+        self._c(lib().ausm_max_wave_speed(self.h, C.byref(w)))
+        return w.value
+
+    def forces(self, with_cp: bool = False):
+        out = np.zeros(6)
+        cp = np.zeros(self.M) if with_cp else None
+        self._c(lib().ausm_forces(self.h, _dp(out), _dp(cp) if cp is not None else None))
+        d = dict(zip(("Fx", "Fy", "F", "Cl", "Cd", "ClCd"), out.tolist()))
+        if with_cp:
+            d["Cp"] = cp
+        return d
+
+    def residual_l2(self) -> float:
+        r = C.c_double()
+        self._c(lib().ausm_residual_l2(self.h, C.byref(r)))
+        return r.value
+
+    def field(self, kind: str = "density") -> np.ndarray:
+        a = np.zeros((self.N, self.M), dtype=np.float32)
+        self._c(lib().ausm_field(self.h, _lib.FIELDS[kind], _fp(a)))
+        return a
+
+    def synchronize(self):
+        self._c(lib().ausm_synchronize(self.h))
+
+    def time_steps(self, n: int, reps: int) -> float:
+        """Device time (ms) of `reps` calls of step(n), CUDA events on the solver's stream."""
+        ms = C.c_float()
+        self._c(lib().ausm_time_steps(self.h, int(n), int(reps), C.byref(ms)))
+        return ms.value

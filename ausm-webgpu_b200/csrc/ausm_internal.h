@@ -1,0 +1,85 @@
+// Internal declarations shared by the CUDA kernels and the C-ABI layer.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <algorithm>
+
+#include "physics.cuh"
+
+namespace ausm {
+
+// Block sizes must be multiples of 32 threads.
+// Block-wide max of non-negative float bit patterns (u32 order == float order for
+// x >= 0; NaN bit patterns compare above +inf, so a NaN wave speed propagates and the
+// host reports divergence).  One atomicMax per block into *dst.  All threads call it.
+__device__ __forceinline__ void block_max_to(uint32_t* dst, uint32_t v) {
+  __shared__ uint32_t warp_max[32];
+  v = __reduce_max_sync(0xffffffffu, v);
+  const int t = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+  const int lane = t & 31, w = t >> 5;
+  if (lane == 0) warp_max[w] = v;
+  __syncthreads();
+  if (w == 0) {
+    const int nw = (blockDim.x * blockDim.y * blockDim.z + 31) >> 5;
+    uint32_t x = lane < nw ? warp_max[lane] : 0u;
+    x = __reduce_max_sync(0xffffffffu, x);
+    if (lane == 0) atomicMax(dst, x);
+  }
+}
+
+// Block-wide sum of doubles into dst (one atomicAdd per block).  All threads call it.
+__device__ __forceinline__ void block_sum_to(double* dst, double v) {
+  __shared__ double warp_sum[32];
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  const int t = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+  const int lane = t & 31, w = t >> 5;
+  if (lane == 0) warp_sum[w] = v;
+  __syncthreads();
+  if (w == 0) {
+    const int nw = (blockDim.x * blockDim.y * blockDim.z + 31) >> 5;
+    double x = lane < nw ? warp_sum[lane] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+    if (lane == 0) atomicAdd(dst, x);
+  }
+}
+
+// ---- fused engine (kernels_fused.cu) ----
+// stage 1..3: RK stage; stage 0: write dQ/dt of Qs to Qo.  emit (stage 3 only):
+// atomicMax the new state's wave speed bits into *wave (zeroed by the caller).
+void launch_fused_stage(int scheme, int stage, bool emit, const float4* Qs, const float4* Qn, float4* Qo,
+                        const float2* V, const float* dt, uint32_t* wave, const Consts& c, int M, int N,
+                        cudaStream_t s);
+void launch_wave_interior(const float4* Q, const float2* V, float gamma, int M, int N, uint32_t* wave,
+                          cudaStream_t s);
+
+// ---- reference-shaped engine (kernels_reference.cu, built with -fmad=false) ----
+// States use the reference layout [N+3][M] (row 0 wall ghost).
+void launch_ref_metrics(const float2* V, float* area, float4* flen, int M, int N, cudaStream_t s);
+void launch_ref_boundary(const float4* in, float4* out, const float2* V, const Consts& c, int M, int N,
+                         cudaStream_t s);
+void launch_ref_fluxes(int scheme, const float4* st, const float2* V, float4* fx, float4* fy, const Consts& c, int M,
+                       int N, cudaStream_t s);
+void launch_ref_residual(const float4* fx, const float4* fy, const float4* flen, const float* area, float4* res, int M,
+                         int N, cudaStream_t s);
+void launch_ref_rk(int stage, const float4* res, const float4* s0, const float4* s1, float4* out, const float* dt,
+                   int M, int N, cudaStream_t s);
+void launch_ref_wave(const float4* st, const float4* flen, const float* area, float gamma, int M, int N,
+                     uint32_t* wave, cudaStream_t s);
+void launch_dt(const uint32_t* wave, float* dt, float maxdt, float cfl, cudaStream_t s);
+
+// ---- grid, layout, forces, norms (kernels_misc.cu) ----
+void launch_to_ref_layout(const float4* Qint, float4* ref, const float2* V, const Consts& c, int M, int N,
+                          cudaStream_t s);
+void launch_from_ref_layout(const float4* ref, float4* Qint, int M, int N, cudaStream_t s);
+void launch_fill(float4* Q, float4 v, size_t n, cudaStream_t s);
+void launch_grid_init(float2* V, int M, int N, double first_spacing, cudaStream_t s);
+void launch_grid_jacobi(const float2* src, float2* dst, int M, int N, cudaStream_t s);
+void launch_grid_multicolor(float2* V, int M, int N, int color, float omega, uint32_t* move, cudaStream_t s);
+void launch_forces(const float4* row0, const float2* V, const Consts& c, int M, double* acc /*2*/, double* cp,
+                   double q_inf, double p_inf, cudaStream_t s);
+void launch_sumsq_rho(const float4* R, size_t n, double* acc, cudaStream_t s);
+void launch_field(const float4* Qint, const float2* V, const Consts& c, int kind, int M, int N, float* out,
+                  cudaStream_t s);
+
+}  // namespace ausm

@@ -1,0 +1,278 @@
+// Device arithmetic of the AUSM-family solver: primitive conversion, ghost cells,
+// MUSCL/van Albada interface states and the SLAU2 / SLAU / AUSM+-up fluxes.
+//
+// Every function takes a template flag FAST.  FAST=false spells each operation as
+// the reference writes it (IEEE division and square root, same operation order); the
+// reference-shaped engine is compiled with -fmad=false so it reproduces the CPU oracle
+// bit for bit.  FAST=true is the fused engine's arithmetic: approximate reciprocal
+// and square root (MUFU, <= 2 ulp), shared reciprocals and an algebraically equal
+// van Albada form; its parity bound against the oracle is tested at 1e-5.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace ausm {
+
+// Per-solve constants, f32 like the reference's uniform buffer (util.js:1-29).  The
+// derived values are computed on the host in f32 in the reference's operation order.
+struct Consts {
+  float gamma, gm1, gm1inv, inRho, inP, Kp, Ku, cfl, maxdt;
+  float2 inflow;   // uni.inflowV
+  float4 inState;  // uni.inState
+  float a2inf;     // (gamma*inP)/inRho                  ausm.js:81
+  float Minf2;     // dot(inflow,inflow)/a2inf            ausm.js:83
+  float Vinf2;     // dot(inflow,inflow)                  ausm.js:273
+  float gammaInP;  // gamma*inP                           ausm.js:273
+  float aStarK;    // (2*gm1)/(gamma+1)                   ausm.js:278
+  float ambE;      // inP/(gamma-1)                       ausm.js:108
+  float gmgm1;     // gamma/(gamma-1), fast enthalpy form (FAST only)
+  int muscl;
+};
+
+template <bool FAST> __device__ __forceinline__ float fdiv(float a, float b) {
+  if constexpr (FAST) return __fdividef(a, b);
+  else return a / b;
+}
+template <bool FAST> __device__ __forceinline__ float frcp(float b) {
+  if constexpr (FAST) return __fdividef(1.0f, b);
+  else return 1.0f / b;
+}
+template <bool FAST> __device__ __forceinline__ float fsqrt(float a) {
+  if constexpr (FAST) {
+    float r;
+    asm("sqrt.approx.f32 %0, %1;" : "=f"(r) : "f"(a));
+    return r;
+  } else {
+    return sqrtf(a);
+  }
+}
+__device__ __forceinline__ float sat(float x) { return fminf(fmaxf(x, 0.0f), 1.0f); }
+__device__ __forceinline__ float wsign(float x) { return x > 0.0f ? 1.0f : (x < 0.0f ? -1.0f : 0.0f); }
+
+// unit normal (-t.y, t.x) of the tangent t = normalize(a - b), and |a - b|
+template <bool FAST>
+__device__ __forceinline__ void edge_normal(float2 a, float2 b, float& nx, float& ny, float& len) {
+  float dx = a.x - b.x, dy = a.y - b.y;
+  float l2 = dx * dx + dy * dy;
+  if constexpr (FAST) {
+    float ri = rsqrtf(l2);
+    len = l2 * ri;
+    float tx = dx * ri, ty = dy * ri;
+    nx = -ty; ny = tx;
+  } else {
+    len = sqrtf(l2);
+    float tx = dx / len, ty = dy / len;
+    nx = -ty; ny = tx;
+  }
+}
+
+// toPrimitive (ausm.js:145-150): (rho, u, v, p), p >= 1e-7
+template <bool FAST> __device__ __forceinline__ float4 to_prim(float4 Q, float gm1) {
+  float rho = Q.x, u, v;
+  if constexpr (FAST) {
+    float ir = frcp<true>(rho);
+    u = Q.y * ir; v = Q.z * ir;
+  } else {
+    u = Q.y / rho; v = Q.z / rho;
+  }
+  float p = fmaxf(1e-7f, (Q.w - 0.5f * rho * (u * u + v * v)) * gm1);
+  return make_float4(rho, u, v, p);
+}
+
+// Wall ghost (ausm.js:57-64): velocity of the first interior cell reflected about the
+// wall normal of the face between vertices a=(i,0), b=(i+1,0); rho and rhoE kept.
+template <bool FAST> __device__ __forceinline__ float4 wall_ghost(float4 s, float2 a, float2 b) {
+  float nx, ny, len;
+  edge_normal<FAST>(a, b, nx, ny, len);
+  float rho = s.x;
+  float u = fdiv<FAST>(s.y, rho), v = fdiv<FAST>(s.z, rho);
+  float dn = 2.0f * (nx * u + ny * v);
+  float gu = u - dn * nx, gv = v - dn * ny;
+  return make_float4(rho, gu * rho, gv * rho, s.w);
+}
+
+// Far-field ghosts (ausm.js:65-117) from the last interior cell s and the outer face
+// between vertices a=(i,N), b=(i+1,N).  g1 = row N+1, g2 = row N+2.
+template <bool FAST>
+__device__ __forceinline__ void far_ghosts(float4 s, float2 a, float2 b, const Consts& c, float4& g1, float4& g2) {
+  float nx, ny, len;
+  edge_normal<FAST>(a, b, nx, ny, len);
+  float rho = s.x;
+  float u = fdiv<FAST>(s.y, rho), v = fdiv<FAST>(s.z, rho);
+  float inout = nx * c.inflow.x + ny * c.inflow.y;
+  if (inout < 0.0f) {  // inflow
+    g1 = c.inState;
+    g2 = c.inState;
+    return;
+  }
+  const float g = c.gamma;
+  float u2 = u * u + v * v;
+  float P = (s.w - 0.5f * u2 * rho) * (g - 1.0f);
+  float a2 = fdiv<FAST>(g * P, rho);
+  float Mint = fdiv<FAST>(u2, a2);
+  if (Mint < 1.0f && c.Minf2 < 1.0f) {  // subsonic: Riemann invariants
+    float un_int = u * nx + v * ny;
+    float a_int = fsqrt<FAST>(a2), a_inf = fsqrt<FAST>(c.a2inf);
+    float J_int = un_int + 2.0f * a_int * c.gm1inv;
+    float J_ext = inout - 2.0f * a_inf * c.gm1inv;
+    float un_g = 0.5f * (J_int + J_ext);
+    float a_g = fmaxf(a_int * 0.1f, 0.25f * (J_int - J_ext) * (g - 1.0f));
+    float X = fmaxf(1e-6f, fdiv<FAST>(a_g, a_int));
+    float X2 = X * X;
+    float rho_g = fmaxf(1e-6f, rho * X2 * X2 * X);
+    float dun = un_g - un_int;
+    float vgx = dun * nx + u, vgy = dun * ny + v;
+    float E_g = fmaxf(1e-6f, fdiv<FAST>(rho_g * a_g * a_g, g)) * c.gm1inv + 0.5f * rho_g * (vgx * vgx + vgy * vgy);
+    g1 = make_float4(rho_g, vgx * rho_g, vgy * rho_g, E_g);
+  } else if (c.Minf2 > 1.0f) {  // ambient pressure
+    g1 = make_float4(s.x, s.y, s.z, c.ambE + 0.5f * rho * u2);
+  } else {  // supersonic outflow: copy
+    g1 = s;
+  }
+  g2 = make_float4(2.0f * g1.x - s.x, 2.0f * g1.y - s.y, 2.0f * g1.z - s.z, 2.0f * g1.w - s.w);
+}
+
+// van Albada-limited MUSCL update of one primitive component (ausm.js:238-249).
+template <bool FAST>
+__device__ __forceinline__ void muscl1(float l2, float l, float r, float r2, float& lo, float& ro) {
+  const float eps = 1e-6f;
+  float dL = l - l2, dF = r - l, dR = r2 - r;
+  float den = dF * dF + eps;
+  float nL = dL * dF + eps, nR = dF * dR + eps;
+  if constexpr (FAST) {
+    // phi(n/d) = (r^2 + r)/(r^2 + 1) = n (n + d) / (n^2 + d^2) with r = n/d: one
+    // reciprocal per side and no division for r itself.
+    float d2 = den * den;
+    float qL = nL * nL + d2, qR = nR * nR + d2;
+    float phiL = nL * (nL + den) * frcp<true>(qL);
+    float phiR = nR * (nR + den) * frcp<true>(qR);
+    lo = l + 0.5f * phiL * dF;
+    ro = r - 0.5f * phiR * dF;
+  } else {
+    float rL = nL / den, rR = nR / den;
+    float r2L = rL * rL, r2R = rR * rR;
+    lo = l + 0.5f * ((r2L + rL) / (r2L + 1.0f)) * dF;
+    ro = r - 0.5f * ((r2R + rR) / (r2R + 1.0f)) * dF;
+  }
+}
+
+// Flux per unit face length through a face with unit normal (nx, ny) pointing from
+// L to R, from the primitive states of the four cells along the face normal line
+// (fluxInterfaceStateCode ausm.js:201-266 + SLAUFluxShaderCode ausm.js:348-391 /
+// AUSMupFluxShaderCode ausm.js:273-334).
+template <int SCHEME, bool FAST>
+__device__ __forceinline__ float4 face_flux(float4 L2, float4 L, float4 R, float4 R2, float nx, float ny,
+                                            const Consts& c) {
+  float4 Lm = L, Rm = R;
+  if (c.muscl > 0) {
+    muscl1<FAST>(L2.x, L.x, R.x, R2.x, Lm.x, Rm.x);
+    muscl1<FAST>(L2.y, L.y, R.y, R2.y, Lm.y, Rm.y);
+    muscl1<FAST>(L2.z, L.z, R.z, R2.z, Lm.z, Rm.z);
+    muscl1<FAST>(L2.w, L.w, R.w, R2.w, Lm.w, Rm.w);
+  }
+  const float gm1 = c.gm1;
+  float rhoL = Lm.x, rhoR = Rm.x, pL = Lm.w, pR = Rm.w;
+  float vxL = Lm.y, vyL = Lm.z, vxR = Rm.y, vyR = Rm.z;
+  float uL = vxL * nx + vyL * ny, uR = vxR * nx + vyR * ny;
+  float kL = vxL * vxL + vyL * vyL, kR = vxR * vxR + vyR * vyR;
+  float hL, hR, irL = 0.0f, irR = 0.0f;
+  if constexpr (FAST) {
+    irL = frcp<true>(rhoL); irR = frcp<true>(rhoR);
+    hL = c.gmgm1 * pL * irL + 0.5f * kL;
+    hR = c.gmgm1 * pR * irR + 0.5f * kR;
+  } else {
+    hL = pL / (gm1 * rhoL) + 0.5f * kL + pL / rhoL;
+    hR = pR / (gm1 * rhoR) + 0.5f * kR + pR / rhoR;
+  }
+  float mdot, P;
+  if constexpr (SCHEME == 2) {  // AUSM+-up, Liou 2006 eqs. 28-30, 69-76
+    float Minf2 = fdiv<FAST>(c.Vinf2, fdiv<FAST>(c.gammaInP, rhoL));
+    const float sigma = 1.0f;
+    float ht = 0.5f * (hL + hR);
+    float aStar = fsqrt<FAST>(fmaxf(1e-6f, c.aStarK * ht));
+    float as2 = aStar * aStar;
+    float aHL = fdiv<FAST>(as2, fmaxf(uL, aStar));
+    float aHR = fdiv<FAST>(as2, fmaxf(-uR, aStar));
+    float a = fminf(aHL, aHR);
+    float ia = frcp<FAST>(a);
+    float ML, MR;
+    if constexpr (FAST) { ML = uL * ia; MR = uR * ia; } else { ML = uL / a; MR = uR / a; }
+    float a2 = a * a;
+    float Mbar2 = fdiv<FAST>(uL * uL + uR * uR, a2 * 2.0f);
+    float Mo2 = fminf(1.0f, fmaxf(Mbar2, Minf2));
+    float fa = Mo2 * (2.0f - Mo2);
+    float rhoI = 0.5f * (rhoL + rhoR);
+    float Mp1L = ML + 1.0f, Mp1R = MR + 1.0f, Mm1L = ML - 1.0f, Mm1R = MR - 1.0f;
+    float M2pL = 0.25f * Mp1L * Mp1L, M2pR = 0.25f * Mp1R * Mp1R;
+    float M2mL = -0.25f * Mm1L * Mm1L, M2mR = -0.25f * Mm1R * Mm1R;
+    bool supL = 1.0f <= fabsf(ML), supR = 1.0f <= fabsf(MR);
+    float M4L = supL ? fmaxf(0.0f, ML) : M2pL * (1.0f + 2.0f * M2mL);
+    float M4R = supR ? fminf(0.0f, MR) : M2mR * (1.0f - 2.0f * M2pR);
+    float Mi = M4L + M4R - fdiv<FAST>(c.Kp / fa * fmaxf(1.0f - sigma * Mbar2, 0.0f) * (pR - pL), rhoI * a2);
+    float alpha4 = 0.75f * (-4.0f + 5.0f * fa * fa);
+    float P5L = supL ? (0.0f <= ML ? 1.0f : 0.0f) : M2pL * ((2.0f - ML) + alpha4 * ML * M2mL);
+    float P5R = supR ? (0.0f <= -MR ? 1.0f : 0.0f) : M2mR * ((-2.0f - MR) - alpha4 * MR * M2pR);
+    P = (P5L * pL + P5R * pR) - c.Ku * P5L * P5R * (rhoL + rhoR) * fa * a * (uR - uL);
+    mdot = a * Mi * (Mi > 0.0f ? rhoL : rhoR);
+  } else {  // SLAU2 (SCHEME 0, Kitamura-Shima 2013) / SLAU (SCHEME 1, Shima-Kitamura 2011)
+    float aL, aR;
+    if constexpr (FAST) {
+      aL = fsqrt<true>(c.gamma * fmaxf(pL, 1e-10f) * frcp<true>(fmaxf(rhoL, 1e-10f)));
+      aR = fsqrt<true>(c.gamma * fmaxf(pR, 1e-10f) * frcp<true>(fmaxf(rhoR, 1e-10f)));
+    } else {
+      aL = sqrtf(c.gamma * fmaxf(pL, 1e-10f) / fmaxf(rhoL, 1e-10f));
+      aR = sqrtf(c.gamma * fmaxf(pR, 1e-10f) / fmaxf(rhoR, 1e-10f));
+    }
+    float a = (aL + aR) * 0.5f;
+    float ia = frcp<FAST>(a);
+    float ML, MR, Uarc, Marc;
+    Uarc = fsqrt<FAST>(0.5f * (kL + kR));
+    if constexpr (FAST) {
+      ML = uL * ia; MR = uR * ia;
+      Marc = fminf(1.0f, Uarc * ia);
+    } else {
+      ML = uL / a; MR = uR / a;
+      Marc = fminf(1.0f, Uarc / a);
+    }
+    float X = (1.0f - Marc) * (1.0f - Marc);
+    float mpL = ML + 1.0f, mmR = MR - 1.0f;
+    float sqL = 0.5f * mpL * mpL, sqR = 0.5f * mmR * mmR;
+    bool supL = 1.0f <= fabsf(ML), supR = 1.0f <= fabsf(MR);
+    float fpp = sat(0.5f * (supL ? 1.0f + 1.0f * wsign(ML) : sqL * (2.0f - 1.0f * ML)));
+    float fpm = sat(0.5f * (supR ? 1.0f + -1.0f * wsign(MR) : sqR * (2.0f - -1.0f * MR)));
+    if constexpr (SCHEME == 0)
+      P = 0.5f * ((fpp - fpm) * (pL - pR) + (pL + pR) + (Uarc * (fpp + fpm - 1.0f) * (rhoL + rhoR) * a));
+    else
+      P = 0.5f * ((fpp - fpm) * (pL - pR) + (1.0f + (1.0f - X) * (fpp + fpm - 1.0f)) * (pL + pR));
+    float dp = pR - pL;
+    float ubar = fdiv<FAST>(rhoL * fabsf(uL) + rhoR * fabsf(uR), rhoL + rhoR);
+    float g = sat(-ML) * sat(MR);
+    float ubp = ubar * (1.0f - g) + fabsf(uL) * g;
+    float ubm = ubar * (1.0f - g) + fabsf(uR) * g;
+    float Xa;
+    if constexpr (FAST) Xa = X * ia; else Xa = X / a;
+    mdot = 0.5f * ((rhoL * (uL + ubp) + rhoR * (uR - ubm)) * (1.0f - g) - Xa * dp);
+  }
+  (void)irL; (void)irR;
+  bool left = mdot > 0.0f;
+  float p1 = left ? vxL : vxR, p2 = left ? vyL : vyR, p3 = left ? hL : hR;
+  return make_float4(1.0f * mdot + 0.0f, p1 * mdot + nx * P, p2 * mdot + ny * P, p3 * mdot + 0.0f);
+}
+
+// Cell wave speed for the CFL condition (ausm.js:617-630): (|v| + a) * sum(l) / (2 A).
+template <bool FAST> __device__ __forceinline__ float wave_speed(float4 s, float lsum, float area, float gamma) {
+  float rho = s.x;
+  float u = fdiv<FAST>(s.y, rho), v = fdiv<FAST>(s.z, rho);
+  float p = (s.w - 0.5f * rho * (u * u + v * v)) * (gamma - 1.0f);
+  float T = fdiv<FAST>(p, rho);
+  float a = fsqrt<FAST>(gamma * T);
+  float speed = fsqrt<FAST>(u * u + v * v);
+  return fdiv<FAST>((speed + a) * lsum, 2.0f * area);
+}
+
+// Cell area of the quad a=(i,j), b=(i+1,j), c=(i,j+1), d=(i+1,j+1) (shaders/grid.js:140).
+__device__ __forceinline__ float quad_area(float2 a, float2 b, float2 c, float2 d) {
+  return 0.5f * fabsf((d.x - a.x) * (c.y - b.y) - (c.x - b.x) * (d.y - a.y));
+}
+
+}  // namespace ausm

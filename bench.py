@@ -1,0 +1,341 @@
+"""Benchmark of the explicit TVD-RK3 O-grid time step (Mcell-updates/s).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (one GPU): NACA 0024 O-grid of 4096 x 3072 cells (12.58 M), circular far field
+at 40 chords, geometric radial stretching with a first cell of 1e-3 chord, M = 6,
+AoA = 4 deg, SLAU2 + MUSCL, TVD-RK3, CFL 0.5, FP32 state, uniform freestream start
+(the large precision-study configuration).  Synthetic: the grid and flow are generated
+here, there is no dataset.  One timed step = one TVD-RK3 step (three fused stage
+launches) of the whole grid; the 201 MB state and 100 MB vertex arrays are larger than
+the 126 MB L2, so every step streams them from HBM.
+
+Multi-GPU (torchrun): every rank advances its own replica of the grid (solves are
+independent; there is no data-path collective), value = all ranks' cell-updates / the
+max over ranks of the device-timed region; scaling is weak.  Host-side timing
+reductions use torch.distributed with the gloo backend.
+
+--impl reference times the reference's own step on the host cores: the reference's
+WGSL compute shaders compiled for the CPU (oracle/_ref, built from the reference
+tree) when present, else the oracle restatement; each step is one RK3 step of a
+sub-grid of the same flow sized so the run ends within a few minutes.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import re
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+sys.path.insert(0, str(ROOT / "ausm-webgpu_b200"))
+
+WORKLOAD = dict(name="naca0024_4096x3072_m6_aoa4_slau2", naca=24, M=4096, N=3072, far_chords=40.0,
+                first_spacing=1e-3, mach=6.0, aoa_deg=4.0, scheme="SLAU2", cfl=0.5, grid_iters=200)
+ALG_BYTES_PER_CELL_STEP = 152  # 3 stages x (16 in + 16 out) + 2 x 16 Qn + 3 x 8 vertex
+METRIC = "Mcell-updates/s per RK3 step"
+
+
+def env_rank():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("LOCAL_RANK", 0)), int(os.environ.get("WORLD_SIZE", 1))
+
+
+def max_over_ranks(x: float, dist=None) -> float:
+    """Max of a host scalar over all ranks (device times are taken as the slowest rank)."""
+    if dist is None or not dist.is_initialized() or dist.get_world_size() == 1:
+        return float(x)
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def traffic_from_profile(cells: int):
+    """Per-launch DRAM bytes of the fused stage kernel from the committed ncu summary."""
+    p = ROOT / "profiles" / "fused_stage_4096x3072.md"
+    if not p.exists():
+        return None
+    m = re.search(r"dram_bytes_per_cell_launch:\s*([0-9.eE+-]+)", p.read_text())
+    if not m:
+        return None
+    return float(m.group(1)) * cells
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.proc = None
+        self.f = None
+
+    def __enter__(self):
+        try:
+            self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-i", str(self.idx), "-lms", "200"], stdout=self.f,
+                                         stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.f:
+            return None
+        try:
+            rows = [r.split(",") for r in Path(self.f.name).read_text().strip().splitlines() if r.strip()]
+            os.unlink(self.f.name)
+        except OSError:
+            return None
+        rows = [[x.strip() for x in r] for r in rows if len(r) >= 9]
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if v.lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def build_solver(ausm, wl, engine="fused", M=None, N=None):
+    M = M or wl["M"]
+    N = N or wl["N"]
+    s = ausm.Solver(M, N, engine=engine)
+    size = 0.5  # half chord: chord 1 centred at the origin
+    s.set_body_naca4(wl["naca"], size, 0.0)
+    s.set_outer_circle(wl["far_chords"] * 2 * size)
+    s.set_radial_stretch(wl["first_spacing"] * 2 * size)
+    s.generate_grid(wl["grid_iters"], "multicolor")
+    s.set_params(gamma=1.4, in_rho=1.0, in_pressure=1.0 / 1.4, mach=wl["mach"], aoa_deg=wl["aoa_deg"], K_p=0.0,
+                 K_u=0.75, cfl=wl["cfl"], maxdt=math.inf, muscl=1, scheme=wl["scheme"], ramp=0.0)
+    s.prepare_state("freestream")
+    return s
+
+
+def cpu_reference_sample(wl, vertices=None, target_s=20.0, K=1):
+    """Time the reference's step on the host cores (oracle/_ref, else the oracle port)."""
+    import numpy as np
+    from oracle.oracle import Oracle, RefWGSL, make_params, oracle_lib, ref_available
+    from oracle.geometry_ref import naca4_boundary, circular_outer
+    kind = "reference" if ref_available() else "port"
+    p = make_params(mach=wl["mach"], aoa_deg=wl["aoa_deg"], scheme=wl["scheme"], cfl=wl["cfl"])
+
+    def make(M, N, verts):
+        if verts is None:
+            o = Oracle(M, N, "f32")
+            v = np.zeros((N + 1, M, 2), np.float32)
+            v[0] = naca4_boundary(M, wl["naca"], 0.5, 0.0)
+            v[N] = circular_outer(M, wl["far_chords"])
+            o.set_vertices(v)
+            o.grid_interpolate()
+            verts = o.vertices()
+            o.close()
+        if kind == "reference":
+            r = RefWGSL(M, N)
+            r.set_uniforms(p)
+            r.set_grid(verts)
+            r.prepare_state(1)
+            return r, r.frame
+        o = Oracle(M, N, "f32")
+        o.set_params(p)
+        o.set_vertices(verts)
+        o.metrics()
+        o.init_state(1)
+        return o, o.step
+
+    # probe the host rate on a small grid, then size the sample
+    obj, fn = make(256, 192, None)
+    t = time.perf_counter()
+    fn(1)
+    rate = 256 * 192 / (time.perf_counter() - t)
+    del obj
+    cells_budget = rate * target_s / max(K, 1)
+    if vertices is not None and wl["M"] * wl["N"] <= cells_budget:
+        M, N, verts = wl["M"], wl["N"], vertices
+    else:
+        scale = max(min(math.sqrt(cells_budget / (wl["M"] * wl["N"])), 1.0), 1 / 32)
+        M = max(32, int(wl["M"] * scale) // 4 * 4)
+        N = max(24, int(wl["N"] * scale) // 3 * 3)
+        verts = None
+    obj, fn = make(M, N, verts)
+    return kind, M, N, fn, obj
+
+
+def threads_used():
+    try:
+        from oracle.oracle import oracle_lib
+        return int(oracle_lib().orc_num_threads())
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def run_reference_arm(args):
+    rank, local_rank, world = env_rank()
+    if rank != 0:
+        return 0
+    wl = WORKLOAD
+    target = max(10.0, min(150.0, 0.15 * args.steps))
+    kind, M, N, fn, obj = cpu_reference_sample(wl, None, target_s=target, K=args.steps + args.warmup)
+    for _ in range(args.warmup):
+        fn(1)
+    t = time.perf_counter()
+    for _ in range(args.steps):
+        fn(1)
+    el = time.perf_counter() - t
+    value = M * N * args.steps / el / 1e6
+    sample = f"{args.steps} RK3 steps of a {M}x{N} O-grid of the same flow (NACA 00{wl['naca']:02d}, M {wl['mach']}, " \
+             f"AoA {wl['aoa_deg']}, {wl['scheme']})"
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "Mcell-updates/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": el / args.steps * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": wl["name"], "sample_grid": f"{M}x{N}", "parallelism": "host cores"},
+            "cpu_baseline": {"value": value, "unit": "Mcell-updates/s", "cores": threads_used(), "kind": kind,
+                             "sample": sample},
+            "e2e": {"value": value, "unit": "Mcell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--engine", default="fused", choices=["fused", "reference"])
+    ap.add_argument("--e2e-calls", type=int, default=5)
+    ap.add_argument("--e2e-steps", type=int, default=100)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--small", action="store_true", help="512x384 grid (profiling and quick checks)")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    if args.impl == "reference":
+        return run_reference_arm(args)
+
+    rank, local_rank, world = env_rank()
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
+
+    import numpy as np
+    import ausm
+    ausm.set_device(local_rank)
+    wl = dict(WORKLOAD)
+    if args.small:
+        wl.update(M=512, N=384, name="naca0024_512x384_m6_aoa4_slau2")
+    s = build_solver(ausm, wl, engine=args.engine)
+    M, N = s.M, s.N
+    cells = M * N
+
+    for _ in range(args.warmup):
+        s.step(1, wait=False)
+    s.synchronize()
+    if dist:
+        dist.barrier()
+    with Clocks(local_rank) as clk:
+        t0 = time.perf_counter()
+        ms = s.time_steps(1, args.steps)  # CUDA events on the solver's stream, synchronised
+        wall = time.perf_counter() - t0
+    clocks = clk.summary()
+    dt_check = s.step(0)  # raises if the run diverged
+    times = [ms]
+    ms = max_over_ranks(ms, dist)
+    value = world * cells * args.steps / (ms * 1e-3) / 1e6
+
+    # end to end through the public API with pinned host buffers
+    e2e = None
+    try:
+        import torch
+        host = torch.empty(((N + 3), M, 4), dtype=torch.float32, pin_memory=True).numpy()
+    except Exception:
+        host = np.empty(((N + 3), M, 4), dtype=np.float32)
+    s.state(out=host)
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.e2e_calls):
+        s.set_state(host)
+        s.step(args.e2e_steps)
+        s.forces(with_cp=True)
+        s.state(out=host)
+    e2e_t = max_over_ranks(time.perf_counter() - t0, dist)
+    state_bytes = (N + 3) * M * 16
+    e2e = {"value": world * cells * args.e2e_steps * args.e2e_calls / e2e_t / 1e6, "unit": "Mcell-updates/s",
+           "h2d_bytes_per_step": state_bytes, "d2h_bytes_per_step": state_bytes + 8 * M + 48 + 8,
+           "step": f"ausm_set_state + ausm_step(n={args.e2e_steps}) + ausm_forces(Cp) + ausm_get_state from/to "
+                   f"pinned host memory", "calls": args.e2e_calls}
+
+    peak, peak_kind = peaks()
+    achieved = cells * ALG_BYTES_PER_CELL_STEP * args.steps / (times[0] * 1e-3) / 1e9
+    traffic = traffic_from_profile(cells)
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": traffic, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind ==
+                "measured" else "fallback 6650 GB/s",
+                "bytes_per_cell_step": ALG_BYTES_PER_CELL_STEP,
+                "kernel": "k_fused_stage (3 launches per RK3 step; achieved over the whole step)"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            verts = s.vertices()
+            kind, cM, cN, fn, obj = cpu_reference_sample(wl, verts, target_s=args.cpu_seconds, K=2)
+            fn(1)
+            t0 = time.perf_counter()
+            fn(2)
+            el = time.perf_counter() - t0
+            cpu = {"value": cM * cN * 2 / el / 1e6, "unit": "Mcell-updates/s", "cores": threads_used(), "kind": kind,
+                   "sample": f"2 RK3 steps of a {cM}x{cN} O-grid of the same flow on the host cores"}
+            del obj
+        except Exception as e:  # the baseline is reported, never required
+            cpu = {"value": None, "unit": "Mcell-updates/s", "cores": None, "kind": None, "sample": f"failed: {e}"}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "Mcell-updates/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": wl["name"], "cells": cells, "grid": f"{M}x{N}", "engine": args.engine,
+                           "parallelism": f"replicas{world}", "l2": "inputs larger than L2 (201 MB state)",
+                           "wall_s": wall},
+                "gpu_launches": (4 if args.engine == "fused" else 17) * args.steps, "clocks": clocks, "roofline": roofline, "cpu_baseline": cpu,
+                "e2e": e2e}
+        print(json.dumps(line))
+    s.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

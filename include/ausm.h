@@ -1,0 +1,174 @@
+/*
+ * libausm — B200 (sm_100a) CUDA library for the explicit TVD-RK3 time step of the
+ * AUSM-family 2-D Euler solver on body-fitted O-grids (huj31415/ausm-webgpu).
+ *
+ * C ABI: plain pointers and sizes, every call returns an int status (AUSM_OK = 0,
+ * negative = error; ausm_last_error() gives the message).  A solver handle owns its
+ * device memory and one CUDA stream; calls on one handle must be serialised by the
+ * caller, distinct handles may be driven from different host threads.
+ *
+ * Each entry point names the reference interface it replaces (file:line inside the
+ * reference project).  The reference exposes its operator surface as browser globals
+ * and hooks (src/main.js, src/util.js, src/grid.js); the mapping is:
+ *   prepareGrid()            main.js:658-705   -> ausm_generate_grid
+ *   prepareState()           main.js:631-655   -> ausm_init_state
+ *   updateSolver(name)       main.js:629       -> ausm_set_scheme
+ *   uni.values.*.set(...)    util.js:162-190   -> ausm_set_params
+ *   frame loop (n steps)     main.js:744-791   -> ausm_step
+ *   forceCalc/Integration    main.js:808-810   -> ausm_forces
+ *   gridVtxData writes       grid.js:267-296   -> ausm_set_body_* / ausm_set_outer / ausm_set_vertices
+ *   state textures           main.js:117-119   -> ausm_get_state / ausm_set_state
+ */
+#ifndef AUSM_H
+#define AUSM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---- */
+#define AUSM_OK 0
+#define AUSM_ERR_INVALID (-1)  /* bad argument or size */
+#define AUSM_ERR_CUDA (-2)     /* CUDA runtime error */
+#define AUSM_ERR_OOM (-3)      /* device allocation failed */
+#define AUSM_ERR_DIVERGED (-4) /* max wave speed or residual norm is NaN/Inf */
+#define AUSM_ERR_STATE (-5)    /* call out of order (no grid or no state yet) */
+#define AUSM_ERR_BUDGET (-6)   /* serving: request does not fit the HBM budget */
+#define AUSM_ERR_TIMEOUT (-7)  /* a bounded device-side wait gave up */
+#define AUSM_ERR_NOT_FOUND (-8) /* serving: unknown request id */
+
+/* flux schemes, in the reference's selector order (util.js:114-118) */
+#define AUSM_SLAU2 0
+#define AUSM_SLAU 1
+#define AUSM_AUSMUP 2
+
+/* initial state: the reference's fluid at rest (ausm.js:1-17) or uniform freestream */
+#define AUSM_INIT_REST 0
+#define AUSM_INIT_FREESTREAM 1
+
+/* outer boundary: the reference's rectangle (grid.js:238-255) or a circle (grid.js:232) */
+#define AUSM_OUTER_RECT 0
+#define AUSM_OUTER_CIRCLE 1
+
+/* elliptic grid iteration: the reference's Jacobi ping-pong (shaders/grid.js:33-110,
+ * main.js:691-694) or multicolour Gauss-Seidel with a converged-move stop */
+#define AUSM_GRID_JACOBI 0
+#define AUSM_GRID_MULTICOLOR 1
+
+/* step engines: one fused kernel per RK stage (default), or the reference's five
+ * dispatches per stage (boundary, j-flux, i-flux, residual, RK combine) */
+#define AUSM_ENGINE_FUSED 0
+#define AUSM_ENGINE_REFERENCE 1
+
+/* headless field outputs (ausm.js:617-707 without colour mapping) */
+#define AUSM_FIELD_DENSITY 0
+#define AUSM_FIELD_PRESSURE 1
+#define AUSM_FIELD_TEMPERATURE 2
+#define AUSM_FIELD_MACH 3
+#define AUSM_FIELD_ENTROPY 4
+#define AUSM_FIELD_WAVE_SPEED 5
+
+/* Physical and numerical parameters: the reference's uniform fields on the path
+ * (util.js:1-29, defaults util.js:78-96, main.js:874-887).  The inflow velocity is
+ * mach * sqrt(gamma * in_pressure / in_rho) rotated by aoa_deg (util.js:180-185); the
+ * inflow state is (rho, rho u, rho v, p/(gamma-1) + rho |V|^2 / 2) (main.js:780-784). */
+typedef struct AusmParams {
+  double gamma;       /* ratio of specific heats (util.js:92) */
+  double in_rho;      /* freestream density (util.js:94) */
+  double in_pressure; /* freestream pressure (util.js:93) */
+  double mach;        /* freestream Mach number */
+  double aoa_deg;     /* angle of attack, degrees (util.js:90) */
+  double K_p;         /* AUSM+-up pressure diffusion (util.js:95) */
+  double K_u;         /* AUSM+-up velocity diffusion (util.js:96) */
+  double cfl;         /* CFL factor (util.js:82) */
+  double maxdt;       /* dt cap; +inf = none (util.js:78) */
+  int muscl;          /* 1 = MUSCL/van Albada reconstruction (main.js:885) */
+  int scheme;         /* AUSM_SLAU2 / AUSM_SLAU / AUSM_AUSMUP */
+  double ramp;        /* inflow ramp strength (util.js:89, main.js:779); 0 = off */
+} AusmParams;
+
+typedef struct ausm_solver ausm_solver;
+
+/* Fills the reference's defaults (util.js:78-96, main.js:877-885). */
+int ausm_default_params(AusmParams* p);
+
+/* Selects the CUDA device that later ausm_create calls on this host thread use
+ * (the library links its own CUDA runtime, so a host's device choice must be passed
+ * here; the reference runs on the browser's one adapter, main.js:9). */
+int ausm_set_device(int device);
+int ausm_device_count(int* count);
+
+/* Creates a solver for an M (around the body, periodic) x N (radial) cell O-grid:
+ * replaces main.js:102-151 (texture allocation).  M >= 4, N >= 2. */
+int ausm_create(int M, int N, ausm_solver** out);
+int ausm_destroy(ausm_solver* h);
+/* Message of the last failed call on h (h == NULL: of the calling thread). */
+const char* ausm_last_error(const ausm_solver* h);
+int ausm_dims(const ausm_solver* h, int* M, int* N);
+
+int ausm_set_engine(ausm_solver* h, int engine);
+int ausm_set_params(ausm_solver* h, const AusmParams* p);   /* util.js:162-190 */
+int ausm_get_params(const ausm_solver* h, AusmParams* p);
+int ausm_set_scheme(ausm_solver* h, int scheme);            /* updateSolver, main.js:629 */
+
+/* Body row j=0, CCW from the trailing edge.  NACA 4-digit formula of grid.js:38-52
+ * (size = half chord, chord centred at x_offset; closed_te=1 keeps the reference's
+ * -0.1036 quartic coefficient, which closes the trailing edge, 0 uses -0.1015). */
+int ausm_set_body_naca4(ausm_solver* h, int digits, double size, double x_offset, int closed_te);
+/* Host-only geometry (no handle, no GPU): the same generators as above, into xy[2*M]. */
+int ausm_naca4_points(int M, int digits, double size, double x_offset, int closed_te, double* xy);
+int ausm_outer_points(int M, int kind, double p0, double p1, double p2, double* xy);
+/* Arbitrary body of exactly M points (a .dat airfoil sampled on the host, airfoilDatParser.js:280). */
+int ausm_set_body_points(ausm_solver* h, const double* xy, int n);
+/* Outer row j=N: AUSM_OUTER_RECT (p0 = half width / half height ratio, grid.js:238-255)
+ * or AUSM_OUTER_CIRCLE (p0 = radius, centre (p1, p2)). */
+int ausm_set_outer(ausm_solver* h, int kind, double p0, double p1, double p2);
+/* Initial guess in j: first_spacing <= 0 is the reference's linear interpolation
+ * (shaders/grid.js:24-27); > 0 is a geometric stretch with that first cell height. */
+int ausm_set_radial_stretch(ausm_solver* h, double first_spacing);
+/* prepareGrid (main.js:658-699): initial guess, `iters` TTM/Winslow sweeps (P=Q=0,
+ * update only where the Jacobian is negative, shaders/grid.js:33-110), then metrics.
+ * AUSM_GRID_MULTICOLOR stops early once the max vertex move is <= tol. */
+int ausm_generate_grid(ausm_solver* h, int iters, int method, double tol, int* iters_done);
+/* Vertices float2 M x (N+1) row-major (main.js:110, grid.js:33). */
+int ausm_set_vertices(ausm_solver* h, const float* xy);
+int ausm_get_vertices(ausm_solver* h, float* xy);
+
+/* prepareState (main.js:631-655): fills the state, then the max wave speed for dt. */
+int ausm_init_state(ausm_solver* h, int mode);
+/* State in the reference layout: float4 (rho, rho u, rho v, rho E) x M x (N+3), row 0 the
+ * wall ghost, rows 1..N interior, rows N+1, N+2 far-field ghosts (main.js:117, util.js:51).
+ * set_state reads the interior rows; get_state writes the interior and the ghost rows
+ * of the boundary pass applied to that interior (ausm.js:34-120). */
+int ausm_set_state(ausm_solver* h, const float* q);
+int ausm_get_state(ausm_solver* h, float* q);
+
+/* step(n): dt = min(maxdt, cfl / max wave speed) of the current state, held for n
+ * TVD-RK3 steps, then the max wave speed of the new state (main.js:744-791).  dt_out
+ * may be NULL (then the call does not wait for the GPU). */
+int ausm_step(ausm_solver* h, int n, float* dt_out);
+int ausm_max_wave_speed(ausm_solver* h, float* out);
+
+/* Surface force (graphs.js:186-272) with FP64 accumulation: out[6] = Fx, Fy,
+ * |F| sign(F.V), Cl, Cd, Cl/Cd (coefficients per the reference, not divided by chord);
+ * cp (may be NULL) gets M wall pressure coefficients (p - p_inf) / q_inf. */
+int ausm_forces(ausm_solver* h, double* out6, double* cp);
+/* sqrt(mean(R_rho^2)) over the interior of the current state, FP64 accumulation. */
+int ausm_residual_l2(ausm_solver* h, double* l2);
+/* Headless field output: M x N floats of AUSM_FIELD_* for the interior. */
+int ausm_field(ausm_solver* h, int kind, float* out);
+
+/* Device stream of the handle (cudaStream_t) and a blocking wait on it. */
+int ausm_stream(ausm_solver* h, void** stream);
+int ausm_synchronize(ausm_solver* h);
+/* Device-timed loop for benchmarks: `reps` calls of step(n) bracketed by CUDA events
+ * on the handle's stream; ms_out gets the elapsed device time of all of them. */
+int ausm_time_steps(ausm_solver* h, int n, int reps, float* ms_out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* AUSM_H */

@@ -15,6 +15,7 @@ Cases (float32 throughout, as the reference's textures):
 """
 from __future__ import annotations
 
+import json
 import sys
 from pathlib import Path
 
@@ -80,6 +81,7 @@ def make():
         out[f"{name}/params"] = np.array([p.gamma, p.in_rho, p.in_pressure, p.inflow[0], p.inflow[1],
                                           *p.in_state, p.K_p, p.K_u, p.cfl, p.maxdt, p.muscl, p.scheme],
                                          dtype=np.float64)
+        out[f"{name}/kw"] = np.array([json.dumps(kw)])
         out[f"{name}/mode"] = np.array([mode])
         out[f"{name}/frames"] = np.array(frames)
         out[f"{name}/maxwave0"] = np.array([r.max_wave()], dtype=np.float32)

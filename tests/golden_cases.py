@@ -25,3 +25,11 @@ def grid_of(g, name):
     gname = str(g[f"{name}/grid"][0])
     M, N = (int(x) for x in g[f"{gname}/meta"][:2])
     return gname, M, N, g[f"{gname}/gridPoints1"]
+
+
+def kwargs_of(g, name) -> dict:
+    """Solver parameters of a case as given to make_params (mach, aoa_deg, scheme, ...)."""
+    import json
+    kw = json.loads(str(g[f"{name}/kw"][0]))
+    kw.setdefault("maxdt", float("inf"))
+    return kw

@@ -1,0 +1,169 @@
+"""CUDA library against the reference (golden fixtures) and the oracle, through the C ABI.
+
+Tolerances:
+  reference-shaped engine (exact arithmetic, -fmad=false): bit-exact state and dt
+  fused engine (approximate MUFU reciprocal/sqrt, FMA): after one RK3 step the max
+    normwise relative difference per conserved component, max|a-b| / max|b|, is
+    <= 1e-5; over longer runs <= 1e-4
+  forces (FP64 accumulation vs the reference's f32 tree sum): 1e-4 relative to |F|
+"""
+import math
+
+import numpy as np
+import pytest
+
+from golden_cases import GRIDS, RUNS, grid_of, kwargs_of
+
+pytestmark = pytest.mark.gpu
+
+TOL_STEP1 = 1e-5
+TOL_RUN = 1e-4
+
+
+def lib_kwargs(kw):
+    """make_params defaults, then the case's overrides, as AusmParams fields."""
+    out = dict(gamma=1.4, in_rho=1.0, in_pressure=1.0 / 1.4, mach=0.5, aoa_deg=0.0, K_p=0.0, K_u=0.75, cfl=0.5,
+               maxdt=math.inf, muscl=1, scheme="SLAU2", ramp=0.0)
+    out.update(kw)
+    return out
+
+
+def normwise(a, b):
+    a = np.asarray(a, np.float64).reshape(-1, 4)
+    b = np.asarray(b, np.float64).reshape(-1, 4)
+    scale = np.maximum(np.abs(b).max(axis=0), 1e-30)
+    return (np.abs(a - b).max(axis=0) / scale).max()
+
+
+def make_solver(golden, name, engine):
+    from ausm import Solver
+    gname, M, N, grid = grid_of(golden, name)
+    s = Solver(M, N, engine=engine)
+    s.set_vertices(grid)
+    s.set_params(**lib_kwargs(kwargs_of(golden, name)))
+    s.prepare_state("rest" if int(golden[f"{name}/mode"][0]) == 0 else "freestream")
+    return s, M, N
+
+
+@pytest.mark.parametrize("name", RUNS)
+def test_reference_engine_bit_exact(golden, name):
+    s, M, N = make_solver(golden, name, "reference")
+    assert np.float32(s.max_wave_speed()) == golden[f"{name}/maxwave0"][0]
+    for k, n in enumerate(golden[f"{name}/frames"]):
+        dt = s.step(int(n))
+        assert np.float32(dt) == golden[f"{name}/dt{k}"][0]
+        q = s.state()
+        ref = golden[f"{name}/state{k}"]
+        assert np.array_equal(q[1:N + 1], ref[1:N + 1]), f"frame {k}: max |diff| {np.abs(q - ref)[1:N + 1].max()}"
+        assert np.float32(s.max_wave_speed()) == golden[f"{name}/maxwave{k + 1}"][0]
+    s.close()
+
+
+@pytest.mark.parametrize("name", RUNS)
+def test_fused_engine_parity(golden, name):
+    s, M, N = make_solver(golden, name, "fused")
+    for k, n in enumerate(golden[f"{name}/frames"]):
+        dt = s.step(int(n))
+        ref_dt = float(golden[f"{name}/dt{k}"][0])
+        tol = TOL_STEP1 if k == 0 and n == 1 else TOL_RUN
+        assert abs(dt - ref_dt) <= tol * ref_dt
+        q = s.state()
+        err = normwise(q[1:N + 1], golden[f"{name}/state{k}"][1:N + 1])
+        assert err <= tol, f"frame {k} ({n} steps): normwise error {err:.3e} > {tol}"
+    s.close()
+
+
+@pytest.mark.parametrize("engine", ["fused", "reference"])
+@pytest.mark.parametrize("name", ["run_slau2_m05_a2_fs", "run_ausmup_m8_a0_fs", "run_slau_m6_odd"])
+def test_forces_and_residual(golden, name, engine):
+    s, M, N = make_solver(golden, name, engine)
+    for n in golden[f"{name}/frames"]:
+        s.step(int(n))
+    f = s.forces(with_cp=True)
+    ref = golden[f"{name}/forces"].astype(np.float64)
+    scale = math.hypot(ref[0], ref[1])
+    assert abs(f["Fx"] - ref[0]) <= 1e-4 * scale and abs(f["Fy"] - ref[1]) <= 1e-4 * scale
+    assert abs(f["Cl"] - ref[3]) <= 1e-4 * max(abs(ref[3]), abs(ref[4]))
+    assert abs(f["Cd"] - ref[4]) <= 1e-4 * max(abs(ref[3]), abs(ref[4]))
+    assert f["Cp"].shape == (M,) and np.all(np.isfinite(f["Cp"]))
+    r_ref = golden[f"{name}/residual"][..., 0].astype(np.float64)
+    l2_ref = math.sqrt(np.mean(r_ref ** 2))
+    tol = 0.0 if engine == "reference" else 1e-3
+    assert abs(s.residual_l2() - l2_ref) <= tol * l2_ref + 1e-12
+    s.close()
+
+
+@pytest.mark.parametrize("gname", GRIDS)
+def test_grid_jacobi_bit_exact(golden, gname):
+    """prepareGrid on the device (Jacobi, -fmad=false) reproduces the reference's grid."""
+    from ausm import Solver
+    M, N, naca, iters = (int(x) for x in golden[f"{gname}/meta"])
+    s = Solver(M, N)
+    s.set_body_points(golden[f"{gname}/body"].astype(np.float64))
+    s.set_outer_rect(1.5)
+    assert s.generate_grid(iters, "jacobi") == iters
+    g = s.vertices()
+    assert np.array_equal(g[N], golden[f"{gname}/outer"])
+    ref = golden[f"{gname}/gridPoints1"]
+    assert np.array_equal(g, ref), f"max |diff| {np.abs(g - ref).max()}"
+    s.close()
+
+
+def test_multicolor_reaches_jacobi_fixed_point():
+    """Multicolour Gauss-Seidel converges to the same discrete TTM grid as Jacobi."""
+    from ausm import Solver
+    from oracle.oracle import Oracle
+    from oracle.geometry_ref import naca4_boundary, rectangular_outer
+    M, N = 48, 16
+    body, outer = naca4_boundary(M, 12, 0.3, -0.7), rectangular_outer(M, 1.5)
+    o = Oracle(M, N, "f64")
+    v = np.zeros((N + 1, M, 2))
+    v[0], v[N] = body.astype(np.float32), outer.astype(np.float32)
+    o.set_vertices(v)
+    o.grid_interpolate()
+    o.grid_jacobi(20000)
+    ref = o.vertices()
+    s = Solver(M, N)
+    s.set_body_points(body)
+    s.set_outer_rect(1.5)
+    s.generate_grid(20000, "multicolor", tol=2e-7)
+    g = s.vertices().astype(np.float64)
+    assert np.abs(g - ref).max() < 1e-4
+    s.close()
+
+
+def test_fused_matches_reference_engine_large():
+    """512 x 384 (README scale): both engines from one grid, 3 steps, SLAU2 M 0.8."""
+    from ausm import Solver
+    M, N = 512, 384
+    res = {}
+    for engine in ("reference", "fused"):
+        s = Solver(M, N, engine=engine)
+        s.set_body_naca4(2412, 0.3, -0.7)
+        s.set_outer_rect(1.5)
+        s.generate_grid(500, "multicolor")
+        s.set_params(**lib_kwargs(dict(mach=0.8, aoa_deg=2.0, cfl=0.5)))
+        s.prepare_state("freestream")
+        s.step(1)
+        res[engine, 1] = s.state()[1:N + 1]
+        s.step(2)
+        res[engine, 3] = s.state()[1:N + 1]
+        s.close()
+    assert normwise(res["fused", 1], res["reference", 1]) <= TOL_STEP1
+    assert normwise(res["fused", 3], res["reference", 3]) <= TOL_RUN
+
+
+def test_symmetric_airfoil_zero_lift():
+    """NACA 0012 at AoA 0 on a mirror-symmetric grid: Cl stays at round-off level."""
+    from ausm import Solver
+    M, N = 256, 128
+    s = Solver(M, N)
+    s.set_body_naca4(12, 0.3, -0.7)
+    s.set_outer_rect(1.5)
+    s.generate_grid(300, "jacobi")
+    s.set_params(**lib_kwargs(dict(mach=0.5, aoa_deg=0.0, cfl=0.5)))
+    s.prepare_state("freestream")
+    s.step(200)
+    f = s.forces()
+    assert abs(f["Cl"]) < 1e-3 * max(abs(f["Cd"]), 1e-3)
+    s.close()
