@@ -47,6 +47,14 @@ template <bool FAST> __device__ __forceinline__ float fsqrt(float a) {
   }
 }
 __device__ __forceinline__ float sat(float x) { return fminf(fmaxf(x, 0.0f), 1.0f); }
+
+// Packed FP32 (sm_100 f32x2): two IEEE-rounded operations per instruction.
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __fadd2_rn(a, make_float2(-b.x, -b.y)); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 lo2(float4 v) { return make_float2(v.x, v.y); }
+__device__ __forceinline__ float2 hi2(float4 v) { return make_float2(v.z, v.w); }
 __device__ __forceinline__ float wsign(float x) { return x > 0.0f ? 1.0f : (x < 0.0f ? -1.0f : 0.0f); }
 
 // unit normal (-t.y, t.x) of the tangent t = normalize(a - b), and |a - b|
@@ -132,6 +140,24 @@ __device__ __forceinline__ void far_ghosts(float4 s, float2 a, float2 b, const C
   g2 = make_float4(2.0f * g1.x - s.x, 2.0f * g1.y - s.y, 2.0f * g1.z - s.z, 2.0f * g1.w - s.w);
 }
 
+// van Albada-limited MUSCL on two primitive components at once (packed f32x2), the
+// FAST form of muscl1: phi(r) = n (n + d) / (n^2 + d^2), r = n / d.
+__device__ __forceinline__ void muscl2_packed(float2 l2, float2 l, float2 r, float2 r2, float2& lo, float2& ro) {
+  const float2 eps = make_float2(1e-6f, 1e-6f), m1 = make_float2(-1.0f, -1.0f);
+  const float2 half = make_float2(0.5f, 0.5f), mhalf = make_float2(-0.5f, -0.5f);
+  // differences as x*(-1) + y: exact products, one rounding, no separate negation
+  float2 dL = fma2(l2, m1, l), dF = fma2(l, m1, r), dR = fma2(r, m1, r2);
+  float2 den = fma2(dF, dF, eps);
+  float2 nL = fma2(dL, dF, eps), nR = fma2(dF, dR, eps);
+  float2 d2 = mul2(den, den);
+  float2 qL = fma2(nL, nL, d2), qR = fma2(nR, nR, d2);
+  float2 rqL = make_float2(__fdividef(1.0f, qL.x), __fdividef(1.0f, qL.y));
+  float2 rqR = make_float2(__fdividef(1.0f, qR.x), __fdividef(1.0f, qR.y));
+  float2 tL = mul2(nL, add2(nL, den)), tR = mul2(nR, add2(nR, den));
+  lo = fma2(mul2(tL, rqL), mul2(half, dF), l);
+  ro = fma2(mul2(tR, rqR), mul2(mhalf, dF), r);
+}
+
 // van Albada-limited MUSCL update of one primitive component (ausm.js:238-249).
 template <bool FAST>
 __device__ __forceinline__ void muscl1(float l2, float l, float r, float r2, float& lo, float& ro) {
@@ -165,10 +191,18 @@ __device__ __forceinline__ float4 face_flux(float4 L2, float4 L, float4 R, float
                                             const Consts& c) {
   float4 Lm = L, Rm = R;
   if (c.muscl > 0) {
-    muscl1<FAST>(L2.x, L.x, R.x, R2.x, Lm.x, Rm.x);
-    muscl1<FAST>(L2.y, L.y, R.y, R2.y, Lm.y, Rm.y);
-    muscl1<FAST>(L2.z, L.z, R.z, R2.z, Lm.z, Rm.z);
-    muscl1<FAST>(L2.w, L.w, R.w, R2.w, Lm.w, Rm.w);
+    if constexpr (FAST) {
+      float2 a, b;
+      muscl2_packed(lo2(L2), lo2(L), lo2(R), lo2(R2), a, b);
+      Lm.x = a.x; Lm.y = a.y; Rm.x = b.x; Rm.y = b.y;
+      muscl2_packed(hi2(L2), hi2(L), hi2(R), hi2(R2), a, b);
+      Lm.z = a.x; Lm.w = a.y; Rm.z = b.x; Rm.w = b.y;
+    } else {
+      muscl1<FAST>(L2.x, L.x, R.x, R2.x, Lm.x, Rm.x);
+      muscl1<FAST>(L2.y, L.y, R.y, R2.y, Lm.y, Rm.y);
+      muscl1<FAST>(L2.z, L.z, R.z, R2.z, Lm.z, Rm.z);
+      muscl1<FAST>(L2.w, L.w, R.w, R2.w, Lm.w, Rm.w);
+    }
   }
   const float gm1 = c.gm1;
   float rhoL = Lm.x, rhoR = Rm.x, pL = Lm.w, pR = Rm.w;
@@ -217,8 +251,10 @@ __device__ __forceinline__ float4 face_flux(float4 L2, float4 L, float4 R, float
   } else {  // SLAU2 (SCHEME 0, Kitamura-Shima 2013) / SLAU (SCHEME 1, Shima-Kitamura 2011)
     float aL, aR;
     if constexpr (FAST) {
-      aL = fsqrt<true>(c.gamma * fmaxf(pL, 1e-10f) * frcp<true>(fmaxf(rhoL, 1e-10f)));
-      aR = fsqrt<true>(c.gamma * fmaxf(pR, 1e-10f) * frcp<true>(fmaxf(rhoR, 1e-10f)));
+      // 1/max(rho, 1e-10) from the already computed 1/rho
+      float igL = rhoL > 1e-10f ? irL : 1e10f, igR = rhoR > 1e-10f ? irR : 1e10f;
+      aL = fsqrt<true>(c.gamma * fmaxf(pL, 1e-10f) * igL);
+      aR = fsqrt<true>(c.gamma * fmaxf(pR, 1e-10f) * igR);
     } else {
       aL = sqrtf(c.gamma * fmaxf(pL, 1e-10f) / fmaxf(rhoL, 1e-10f));
       aR = sqrtf(c.gamma * fmaxf(pR, 1e-10f) / fmaxf(rhoR, 1e-10f));
@@ -238,15 +274,22 @@ __device__ __forceinline__ float4 face_flux(float4 L2, float4 L, float4 R, float
     float mpL = ML + 1.0f, mmR = MR - 1.0f;
     float sqL = 0.5f * mpL * mpL, sqR = 0.5f * mmR * mmR;
     bool supL = 1.0f <= fabsf(ML), supR = 1.0f <= fabsf(MR);
-    float fpp = sat(0.5f * (supL ? 1.0f + 1.0f * wsign(ML) : sqL * (2.0f - 1.0f * ML)));
-    float fpm = sat(0.5f * (supR ? 1.0f + -1.0f * wsign(MR) : sqR * (2.0f - -1.0f * MR)));
+    float fpp, fpm;
+    if constexpr (FAST) {
+      // supersonic branch: 0.5 (1 + sign M) is 1 or 0 (|M| >= 1, so M != 0)
+      fpp = supL ? (ML > 0.0f ? 1.0f : 0.0f) : __saturatef(0.5f * (sqL * (2.0f - ML)));
+      fpm = supR ? (MR > 0.0f ? 0.0f : 1.0f) : __saturatef(0.5f * (sqR * (2.0f + MR)));
+    } else {
+      fpp = sat(0.5f * (supL ? 1.0f + 1.0f * wsign(ML) : sqL * (2.0f - 1.0f * ML)));
+      fpm = sat(0.5f * (supR ? 1.0f + -1.0f * wsign(MR) : sqR * (2.0f - -1.0f * MR)));
+    }
     if constexpr (SCHEME == 0)
       P = 0.5f * ((fpp - fpm) * (pL - pR) + (pL + pR) + (Uarc * (fpp + fpm - 1.0f) * (rhoL + rhoR) * a));
     else
       P = 0.5f * ((fpp - fpm) * (pL - pR) + (1.0f + (1.0f - X) * (fpp + fpm - 1.0f)) * (pL + pR));
     float dp = pR - pL;
     float ubar = fdiv<FAST>(rhoL * fabsf(uL) + rhoR * fabsf(uR), rhoL + rhoR);
-    float g = sat(-ML) * sat(MR);
+    float g = FAST ? __saturatef(-ML) * __saturatef(MR) : sat(-ML) * sat(MR);
     float ubp = ubar * (1.0f - g) + fabsf(uL) * g;
     float ubm = ubar * (1.0f - g) + fabsf(uR) * g;
     float Xa;
