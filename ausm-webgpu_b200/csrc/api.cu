@@ -2,6 +2,7 @@
 // orchestration of the device kernels for the reference's operator surface.
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -37,6 +38,8 @@ struct ausm_solver {
   float* dt = nullptr;
   double* dacc = nullptr;
   uint32_t* move = nullptr;
+  int* err_flag = nullptr;  // set by a kernel whose bounded wait gave up
+  TmaMaps tma;
   float* h_dt = nullptr;
   uint32_t* h_wave = nullptr;
   double* h_acc = nullptr;
@@ -220,7 +223,7 @@ int ausm_destroy(ausm_solver* h) {
   cudaSetDevice(h->dev);
   if (h->st) cudaStreamSynchronize(h->st);
   void* dptrs[] = {h->V, h->V2, h->Q[0], h->Q[1], h->Q[2], h->S[0], h->S[1], h->S[2], h->fx, h->fy, h->res,
-                   h->flen, h->area, h->staging, h->cp, h->wave, h->dt, h->dacc, h->move};
+                   h->flen, h->area, h->staging, h->cp, h->wave, h->dt, h->dacc, h->move, h->err_flag};
   for (void* d : dptrs)
     if (d) cudaFree(d);
   if (h->h_dt) cudaFreeHost(h->h_dt);
@@ -270,11 +273,19 @@ int ausm_create(int M, int N, ausm_solver** out) {
   TRY(dalloc(&h->dt, 4));
   TRY(dalloc(&h->dacc, 4));
   TRY(dalloc(&h->move, 4));
+  TRY(dalloc(&h->err_flag, 1));
+  TRY(cudaMemsetAsync(h->err_flag, 0, sizeof(int), h->st));
   TRY(cudaMallocHost((void**)&h->h_dt, 4 * sizeof(float)));
   TRY(cudaMallocHost((void**)&h->h_wave, 4 * sizeof(uint32_t)));
   TRY(cudaMallocHost((void**)&h->h_acc, 4 * sizeof(double)));
   TRY(cudaMemsetAsync(h->wave, 0, 4 * sizeof(uint32_t), h->st));
 #undef TRY
+  {
+    const float4* qs[3] = {h->Q[0], h->Q[1], h->Q[2]};
+    // odd M keeps the per-thread staging kernel; AUSM_NO_TMA=1 selects it for A/B timing
+    const char* no_tma = std::getenv("AUSM_NO_TMA");
+    if (!(no_tma && no_tma[0] == '1')) encode_tma_maps(qs, h->V, M, N, &h->tma);
+  }
   ausm_default_params(&h->p);
   h->speed_now = inflow_target(h->p);
   make_consts(h);
@@ -585,9 +596,20 @@ int ausm_step(ausm_solver* h, int n, float* dt_out) {
     if (h->engine == AUSM_ENGINE_FUSED) {
       for (int k = 0; k < n; k++) {
         int a = h->cur, b = (a + 1) % 3, c3 = (a + 2) % 3;
-        launch_fused_stage(sch, 1, false, h->Q[a], nullptr, h->Q[b], h->V, h->dt, h->wave, h->c, M, N, s);
-        launch_fused_stage(sch, 2, false, h->Q[b], h->Q[a], h->Q[c3], h->V, h->dt, h->wave, h->c, M, N, s);
-        launch_fused_stage(sch, 3, k == n - 1, h->Q[c3], h->Q[a], h->Q[b], h->V, h->dt, h->wave, h->c, M, N, s);
+        TmaMapsLaunch t1, t2, t3;
+        const TmaMapsLaunch *p1 = nullptr, *p2 = nullptr, *p3 = nullptr;
+        if (h->tma.ok) {
+          t1 = {h->tma.halo[a], h->tma.plain[a], h->tma.v};
+          t2 = {h->tma.halo[b], h->tma.plain[a], h->tma.v};
+          t3 = {h->tma.halo[c3], h->tma.plain[a], h->tma.v};
+          p1 = &t1; p2 = &t2; p3 = &t3;
+        }
+        launch_fused_stage(sch, 1, false, h->Q[a], nullptr, h->Q[b], h->V, h->dt, h->wave, h->c, M, N, p1,
+                           h->err_flag, s);
+        launch_fused_stage(sch, 2, false, h->Q[b], h->Q[a], h->Q[c3], h->V, h->dt, h->wave, h->c, M, N, p2,
+                           h->err_flag, s);
+        launch_fused_stage(sch, 3, k == n - 1, h->Q[c3], h->Q[a], h->Q[b], h->V, h->dt, h->wave, h->c, M, N, p3,
+                           h->err_flag, s);
         h->cur = b;
       }
     } else {
@@ -619,7 +641,12 @@ int ausm_step(ausm_solver* h, int n, float* dt_out) {
   if (dt_out) {
     CU(h, cudaMemcpyAsync(h->h_dt, h->dt, sizeof(float), cudaMemcpyDeviceToHost, s));
     CU(h, cudaMemcpyAsync(h->h_wave, h->wave, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    CU(h, cudaMemcpyAsync(h->h_wave + 2, h->err_flag, sizeof(int), cudaMemcpyDeviceToHost, s));
     CU(h, cudaStreamSynchronize(s));
+    if (h->h_wave[2] != 0) {
+      CU(h, cudaMemsetAsync(h->err_flag, 0, sizeof(int), s));
+      return fail(h, AUSM_ERR_TIMEOUT, "a tile load did not arrive within the bounded wait");
+    }
     *dt_out = h->h_dt[0];
     float w;
     std::memcpy(&w, h->h_wave, 4);
@@ -684,7 +711,7 @@ int ausm_residual_l2(ausm_solver* h, double* l2) {
   if (h->engine == AUSM_ENGINE_FUSED) {
     float4* scratch = h->Q[(h->cur + 1) % 3];
     launch_fused_stage(h->p.scheme, 0, false, h->Q[h->cur], nullptr, scratch, h->V, h->dt, h->wave, h->c, M, N,
-                       h->st);
+                       nullptr, h->err_flag, h->st);
     R = scratch;
   } else {
     launch_ref_boundary(h->S[2], h->S[0], h->V, h->c, M, N, h->st);

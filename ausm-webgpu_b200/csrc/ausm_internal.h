@@ -1,5 +1,6 @@
 // Internal declarations shared by the CUDA kernels and the C-ABI layer.
 #pragma once
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -45,11 +46,26 @@ __device__ __forceinline__ void block_sum_to(double* dst, double v) {
 }
 
 // ---- fused engine (kernels_fused.cu) ----
+// TMA descriptors of one solve: per state buffer the halo box (36 x 20 cells) and the
+// plain box (32 x 16 cells), and the vertex box (34 x 17).
+struct TmaMaps {
+  CUtensorMap halo[3];
+  CUtensorMap plain[3];
+  CUtensorMap v;
+  bool ok = false;
+};
+struct TmaMapsLaunch {  // the three a stage launch reads
+  CUtensorMap qs;
+  CUtensorMap qn;
+  CUtensorMap v;
+};
+bool encode_tma_maps(const float4* const Q[3], const float2* V, int M, int N, TmaMaps* out);
 // stage 1..3: RK stage; stage 0: write dQ/dt of Qs to Qo.  emit (stage 3 only):
-// atomicMax the new state's wave speed bits into *wave (zeroed by the caller).
+// atomicMax the new state's wave speed bits into *wave (zeroed by the caller).  With
+// tm != nullptr the persistent TMA kernel runs and sets *err on a bounded-wait timeout.
 void launch_fused_stage(int scheme, int stage, bool emit, const float4* Qs, const float4* Qn, float4* Qo,
                         const float2* V, const float* dt, uint32_t* wave, const Consts& c, int M, int N,
-                        cudaStream_t s);
+                        const TmaMapsLaunch* tm, int* err, cudaStream_t s);
 void launch_wave_interior(const float4* Q, const float2* V, float gamma, int M, int N, uint32_t* wave,
                           cudaStream_t s);
 

@@ -1,35 +1,51 @@
-// Fused TVD-RK3 stage kernel: one launch per stage does the work of the reference's
+// Fused TVD-RK3 stage kernels: one launch per stage does the work of the reference's
 // five dispatches (boundary ausm.js:23, j-flux + i-flux ausm.js:271/345, residual
 // ausm.js:402, RK stage ausm.js:441/470/501).
 //
-// A CTA of 32 x 8 threads owns a TX=32 x TY=16 tile of interior cells; thread (x, y)
-// owns cells (x, y) and (x, y+8) and keeps their conserved state in registers.  The
-// CTA stages into shared memory
-//   - primitives of the tile plus a 2-cell MUSCL halo on every side (corners
-//     skipped), the periodic seam wrapped in i, and the ghost rows (wall j=-1,-2 and
-//     far field j=N,N+1) computed in place from the interior,
+// Work decomposition (both kernels): a CTA of 32 x 8 threads handles a TX=32 x TY=16
+// tile of interior cells; thread (x, y) owns cells (x, y) and (x, y+8) and keeps their
+// conserved state in registers.  Per tile, shared memory holds
+//   - P: primitives of the tile plus a 2-cell MUSCL halo on every side (corners
+//     unused), the periodic seam wrapped in i and the ghost rows (wall j=-1,-2, far
+//     field j=N,N+1) computed in place from the interior,
 //   - the (TX+1) x (TY+1) vertices of the tile,
-// evaluates every i-face and j-face of the tile exactly once (flux x face length in
-// shared memory; warp w evaluates face rows w and w+8 of each direction, warps 0 and 1
-// the extra top row and right column), then per owned cell assembles the residual and
-// the stage combination and stores the new conserved state as one float4.  The last
-// stage-3 launch of a step(n) call also reduces the new state's CFL wave speed (block
-// max, one atomicMax on the float bits, as cflReductionShaderCode ausm.js:535-581).
+//   - Fi/Fj: flux x length of every i-face and j-face of the tile, each evaluated once
+//     (warp w takes face rows w and w+8 of each direction; warps 0 and 1 also the top
+//     face row and the right face column),
+// and each thread then assembles the residual and the stage combination of its two
+// cells and stores the new conserved states as float4.  The last stage-3 launch of a
+// step(n) call also reduces the new state's CFL wave speed (block max, one atomicMax
+// on the float bits, as cflReductionShaderCode ausm.js:535-581).
+//
+// k_fused_stage_tma (the default when M is even) is persistent: each CTA walks tiles
+// t = blockIdx.x, blockIdx.x + gridDim.x, ... and stages them with TMA
+// (cp.async.bulk.tensor, no multicast) into a double buffer — the next tile's state
+// box (36 x 20 cells with halo) and vertex box load while the current tile computes,
+// and Qn for stages 2 and 3 loads during the face phase.  Out-of-range box columns
+// (the periodic seam) and rows (ghost rows) are filled in by the threads.  Every
+// mbarrier wait is bounded; on a timeout the CTA sets *err and stops.
+// k_fused_stage loads the same tile with per-thread loads (odd M, where the vertex row
+// pitch M*8 bytes is not a multiple of 16 and cannot be a TMA stride).
 //
 // HBM layout: interior state float4 [N][M] (row-major, no ghost rows), vertices
 // float2 [N+1][M].  Algorithmic traffic per cell and stage: 16 B state in, 16 B out,
 // 16 B Qn in (stages 2 and 3), 8 B vertex.
 #include "ausm_internal.h"
+#include "tma.cuh"
 
 namespace ausm {
 
 #ifndef AUSM_FUSED_MIN_BLOCKS
 #define AUSM_FUSED_MIN_BLOCKS 4  // resident CTAs per SM the register budget is sized for
 #endif
+#ifndef AUSM_TMA_MIN_BLOCKS
+#define AUSM_TMA_MIN_BLOCKS 3
+#endif
 
 namespace {
-constexpr int TX = 32, TY = 16, NWX = 32, NWY = 8;
+constexpr int TX = 32, TY = 16, NWX = 32, NWY = 8, NT = NWX * NWY;
 constexpr int PW = TX + 4, PH = TY + 4;
+constexpr int VW_TMA = TX + 2;  // vertex box width: 34 x 8 B = 272 B, a multiple of 16 B
 
 // i in [-2, M + TX + 2) -> [0, M); the last branch only runs for M < TX + 3
 __device__ __forceinline__ int wrap_i(int i, int M) {
@@ -53,33 +69,14 @@ __device__ __forceinline__ float4 tile_cell(const float4* __restrict__ Qs, const
     far_ghosts<true>(__ldg(&Qs[(size_t)(N - 1) * M + i]), __ldg(&V[vb + i]), __ldg(&V[vb + r]), c, g1, g2);
     return j == N ? g1 : g2;
   }
-  return make_float4(1.0f, 0.0f, 0.0f, 1.0f);  // beyond the far field: never read
+  return make_float4(1.0f, 0.0f, 0.0f, 1.0f);  // beyond the far field: never read by a valid face
 }
-}  // namespace
 
-template <int SCHEME, int STAGE, bool EMIT>
-__global__ void __launch_bounds__(NWX* NWY, AUSM_FUSED_MIN_BLOCKS)
-    k_fused_stage(const float4* __restrict__ Qs, const float4* __restrict__ Qn, float4* __restrict__ Qo,
-                  const float2* __restrict__ V, const float* __restrict__ dtp, uint32_t* __restrict__ wave,
-                  const Consts c, const int M, const int N) {
-  __shared__ float4 P[PH][PW];
-  __shared__ float2 Vs[TY + 1][TX + 1];
-  __shared__ float4 Fi[TY][TX + 1];
-  __shared__ float4 Fj[TY + 1][TX];
-
-  const int tx = threadIdx.x, ty = threadIdx.y;
-  const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY;
-  const int ic = wrap_i(i0 + tx, M);  // column of the owned cells (wrapped when i0+tx >= M)
-  const int ja = j0 + ty, jb = j0 + ty + 8;
-
-  // ---- stage the tile ----
-  // owned cells (tile rows ty+2, ty+10, column tx+2), kept in registers
-  const float4 qa = tile_cell(Qs, V, c, M, N, ic, ja);
-  const float4 qb = tile_cell(Qs, V, c, M, N, ic, jb);
-  // halo rows (warps 0-3: rows 0, 1, TY+2, TY+3, columns 2..TX+1) and halo columns
-  // (warps 4-5: columns 0, 1, TX+2, TX+3, rows 2..TY+1)
-  float4 qh = make_float4(1.0f, 0.0f, 0.0f, 1.0f);
-  int hr = -1, hc = -1;
+// halo entry of thread (tx, ty): warps 0-3 take primitive rows 0, 1, TY+2, TY+3
+// (columns 2..TX+1), warps 4-5 columns 0, 1, TX+2, TX+3 (rows 2..TY+1)
+__device__ __forceinline__ void halo_entry(int tx, int ty, int& hr, int& hc) {
+  hr = -1;
+  hc = -1;
   if (ty < 4) {
     hr = ty < 2 ? ty : TY + ty;
     hc = tx + 2;
@@ -89,53 +86,46 @@ __global__ void __launch_bounds__(NWX* NWY, AUSM_FUSED_MIN_BLOCKS)
     hc = sel < 2 ? sel : TX + sel;
     hr = 2 + (k & 15);
   }
-  if (hr >= 0) qh = tile_cell(Qs, V, c, M, N, wrap_i(i0 - 2 + hc, M), j0 - 2 + hr);
-  // vertices: rows ty, ty+8, ty+16 (ty = 0), columns tx and (lane 0) TX
-  for (int r = ty; r <= TY; r += NWY) {
-    int j = j0 + r;
-    if (j <= N) {
-      Vs[r][tx] = __ldg(&V[(size_t)j * M + ic]);
-      if (tx == 0) Vs[r][TX] = __ldg(&V[(size_t)j * M + wrap_i(i0 + TX, M)]);
+}
+
+// Flux x length of every face of the tile.  Vs is the vertex tile with row width VW.
+template <int SCHEME, int VW>
+__device__ __forceinline__ void faces_phase(const float4 (*P)[PW], const float2* Vs, float4 (*Fi)[TX + 1],
+                                            float4 (*Fj)[TX], const Consts& c, int i0, int j0, int M, int N, int tx,
+                                            int ty) {
+  const int nI = ty == 1 && tx < TY ? 3 : 2;
+  for (int t = 0; t < nI; t++) {
+    const int r = t < 2 ? ty + 8 * t : tx;
+    const int cc = t < 2 ? tx : TX;
+    if (j0 + r < N && cc <= M - i0) {
+      float nx, ny, len;
+      edge_normal<true>(Vs[(r + 1) * VW + cc], Vs[r * VW + cc], nx, ny, len);  // tangent V(i,j+1)-V(i,j)
+      const float4* b = &P[r + 2][cc];
+      float4 f = face_flux<SCHEME, true>(b[0], b[1], b[2], b[3], nx, ny, c);
+      Fi[r][cc] = make_float4(f.x * len, f.y * len, f.z * len, f.w * len);
     }
   }
-  P[ty + 2][tx + 2] = to_prim<true>(qa, c.gm1);
-  P[ty + 10][tx + 2] = to_prim<true>(qb, c.gm1);
-  if (hr >= 0) P[hr][hc] = to_prim<true>(qh, c.gm1);
-  __syncthreads();
-
-  // ---- faces: flux x length, each face once ----
-  // i-faces of rows ty and ty+8 (and, on warp 1, the right column TX); j-faces of rows
-  // ty and ty+8 (and, on warp 0, the top row TY).  Strides are compile-time.
-  {
-    const int nI = ty == 1 && tx < TY ? 3 : 2;
-    for (int t = 0; t < nI; t++) {
-      const int r = t < 2 ? ty + 8 * t : tx;
-      const int cc = t < 2 ? tx : TX;
-      if (j0 + r < N && cc <= M - i0) {
-        float nx, ny, len;
-        edge_normal<true>(Vs[r + 1][cc], Vs[r][cc], nx, ny, len);  // tangent V(i,j+1)-V(i,j)
-        const float4* b = &P[r + 2][cc];
-        float4 f = face_flux<SCHEME, true>(b[0], b[1], b[2], b[3], nx, ny, c);
-        Fi[r][cc] = make_float4(f.x * len, f.y * len, f.z * len, f.w * len);
-      }
-    }
-    const int nJ = ty == 0 ? 3 : 2;
-    for (int t = 0; t < nJ; t++) {
-      const int r = t < 2 ? ty + 8 * t : TY;
-      const int cc = tx;
-      if (j0 + r <= N && i0 + cc < M) {
-        float nx, ny, len;
-        edge_normal<true>(Vs[r][cc], Vs[r][cc + 1], nx, ny, len);  // tangent V(i,j)-V(i+1,j)
-        const float4* b = &P[r][cc + 2];
-        float4 f = face_flux<SCHEME, true>(b[0], b[PW], b[2 * PW], b[3 * PW], nx, ny, c);
-        Fj[r][cc] = make_float4(f.x * len, f.y * len, f.z * len, f.w * len);
-      }
+  const int nJ = ty == 0 ? 3 : 2;
+  for (int t = 0; t < nJ; t++) {
+    const int r = t < 2 ? ty + 8 * t : TY;
+    const int cc = tx;
+    if (j0 + r <= N && i0 + cc < M) {
+      float nx, ny, len;
+      edge_normal<true>(Vs[r * VW + cc], Vs[r * VW + cc + 1], nx, ny, len);  // tangent V(i,j)-V(i+1,j)
+      const float4* b = &P[r][cc + 2];
+      float4 f = face_flux<SCHEME, true>(b[0], b[PW], b[2 * PW], b[3 * PW], nx, ny, c);
+      Fj[r][cc] = make_float4(f.x * len, f.y * len, f.z * len, f.w * len);
     }
   }
-  __syncthreads();
+}
 
-  // ---- residual + stage combination for the owned cells ----
-  const float dt = *dtp;
+// Residual and stage combination of the two owned cells; returns the max wave-speed
+// bits of the new state when EMIT.  qn(h) fetches Qn of owned cell h (stages 2, 3).
+template <int STAGE, bool EMIT, int VW, class QnFetch>
+__device__ __forceinline__ uint32_t combine_phase(const float2* Vs, const float4 (*Fi)[TX + 1],
+                                                  const float4 (*Fj)[TX], float4 qa, float4 qb, QnFetch qn,
+                                                  float4* __restrict__ Qo, float dt, const Consts& c, int i0, int j0,
+                                                  int M, int N, int tx, int ty) {
   uint32_t wmax = 0u;
   const int i = i0 + tx;
 #pragma unroll
@@ -144,40 +134,223 @@ __global__ void __launch_bounds__(NWX* NWY, AUSM_FUSED_MIN_BLOCKS)
     const int j = j0 + r;
     if (i < M && j < N) {
       const float4 q = h ? qb : qa;
-      float2 a = Vs[r][tx], b = Vs[r][tx + 1], cv = Vs[r + 1][tx], d = Vs[r + 1][tx + 1];
-      float iA = frcp<true>(quad_area(a, b, cv, d));
+      float2 a = Vs[r * VW + tx], b = Vs[r * VW + tx + 1], cv = Vs[(r + 1) * VW + tx], d = Vs[(r + 1) * VW + tx + 1];
+      float A = quad_area(a, b, cv, d);
+      float iA = frcp<true>(A);
       float4 fl = Fi[r][tx], fr = Fi[r][tx + 1], fd = Fj[r][tx], fu = Fj[r + 1][tx];
       float4 R;
       R.x = -(((fr.x - fl.x) + fu.x) - fd.x) * iA;
       R.y = -(((fr.y - fl.y) + fu.y) - fd.y) * iA;
       R.z = -(((fr.z - fl.z) + fu.z) - fd.z) * iA;
       R.w = -(((fr.w - fl.w) + fu.w) - fd.w) * iA;
-      size_t o = (size_t)j * M + i;
       float4 out;
       if constexpr (STAGE == 0) {  // residual only (dQ/dt)
         out = R;
       } else if constexpr (STAGE == 1) {
         out = make_float4(q.x + dt * R.x, q.y + dt * R.y, q.z + dt * R.z, q.w + dt * R.w);
       } else if constexpr (STAGE == 2) {
-        float4 n = __ldg(&Qn[o]);
+        float4 n = qn(h);
         out = make_float4(0.75f * n.x + 0.25f * (q.x + dt * R.x), 0.75f * n.y + 0.25f * (q.y + dt * R.y),
                           0.75f * n.z + 0.25f * (q.z + dt * R.z), 0.75f * n.w + 0.25f * (q.w + dt * R.w));
       } else {
-        float4 n = __ldg(&Qn[o]);
+        float4 n = qn(h);
         const float third = 1.0f / 3.0f;
         out = make_float4((n.x + 2.0f * (q.x + dt * R.x)) * third, (n.y + 2.0f * (q.y + dt * R.y)) * third,
                           (n.z + 2.0f * (q.z + dt * R.z)) * third, (n.w + 2.0f * (q.w + dt * R.w)) * third);
       }
-      Qo[o] = out;
+      Qo[(size_t)j * M + i] = out;
       if constexpr (EMIT) {
         float ll = sqrtf((a.x - cv.x) * (a.x - cv.x) + (a.y - cv.y) * (a.y - cv.y));
         float lr = sqrtf((b.x - d.x) * (b.x - d.x) + (b.y - d.y) * (b.y - d.y));
         float lu = sqrtf((cv.x - d.x) * (cv.x - d.x) + (cv.y - d.y) * (cv.y - d.y));
         float ld = sqrtf((a.x - b.x) * (a.x - b.x) + (a.y - b.y) * (a.y - b.y));
-        float w = wave_speed<true>(out, ((ll + lr) + lu) + ld, quad_area(a, b, cv, d), c.gamma);
+        float w = wave_speed<true>(out, ((ll + lr) + lu) + ld, A, c.gamma);
         wmax = max(wmax, __float_as_uint(w));
       }
     }
+  }
+  return wmax;
+}
+}  // namespace
+
+// ---- per-thread staging, one tile per CTA ----
+template <int SCHEME, int STAGE, bool EMIT>
+__global__ void __launch_bounds__(NT, AUSM_FUSED_MIN_BLOCKS)
+    k_fused_stage(const float4* __restrict__ Qs, const float4* __restrict__ Qn, float4* __restrict__ Qo,
+                  const float2* __restrict__ V, const float* __restrict__ dtp, uint32_t* __restrict__ wave,
+                  const Consts c, const int M, const int N) {
+  __shared__ float4 P[PH][PW];
+  __shared__ float2 Vs[(TY + 1) * (TX + 1)];
+  __shared__ float4 Fi[TY][TX + 1];
+  __shared__ float4 Fj[TY + 1][TX];
+
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY;
+  const int ic = wrap_i(i0 + tx, M);  // column of the owned cells (wrapped when i0+tx >= M)
+
+  const float4 qa = tile_cell(Qs, V, c, M, N, ic, j0 + ty);
+  const float4 qb = tile_cell(Qs, V, c, M, N, ic, j0 + ty + 8);
+  int hr, hc;
+  halo_entry(tx, ty, hr, hc);
+  float4 qh = make_float4(1.0f, 0.0f, 0.0f, 1.0f);
+  if (hr >= 0) qh = tile_cell(Qs, V, c, M, N, wrap_i(i0 - 2 + hc, M), j0 - 2 + hr);
+  for (int r = ty; r <= TY; r += NWY) {  // vertices: rows ty, ty+8, ty+16; columns tx and TX
+    int j = j0 + r;
+    if (j <= N) {
+      Vs[r * (TX + 1) + tx] = __ldg(&V[(size_t)j * M + ic]);
+      if (tx == 0) Vs[r * (TX + 1) + TX] = __ldg(&V[(size_t)j * M + wrap_i(i0 + TX, M)]);
+    }
+  }
+  P[ty + 2][tx + 2] = to_prim<true>(qa, c.gm1);
+  P[ty + 10][tx + 2] = to_prim<true>(qb, c.gm1);
+  if (hr >= 0) P[hr][hc] = to_prim<true>(qh, c.gm1);
+  __syncthreads();
+
+  faces_phase<SCHEME, TX + 1>(P, Vs, Fi, Fj, c, i0, j0, M, N, tx, ty);
+  __syncthreads();
+
+  auto qn = [&](int h) { return __ldg(&Qn[(size_t)(j0 + ty + 8 * h) * M + i0 + tx]); };
+  uint32_t wmax = combine_phase<STAGE, EMIT, TX + 1>(Vs, Fi, Fj, qa, qb, qn, Qo, *dtp, c, i0, j0, M, N, tx, ty);
+  if constexpr (EMIT) block_max_to(wave, wmax);
+}
+
+// ---- persistent TMA-staged version ----
+namespace {
+// dynamic shared memory layout (offsets multiples of 128 B)
+constexpr int SQ_BYTES = PH * PW * 16;                 // 11520: state box (36 x 20 float4)
+constexpr int SV_BYTES = (TY + 1) * VW_TMA * 8;        // 4624:  vertex box (34 x 17 float2)
+constexpr int SN_BYTES = TY * TX * 16;                 // 8192:  Qn box (32 x 16 float4)
+constexpr int r128(int x) { return (x + 127) / 128 * 128; }
+constexpr int OFF_Q0 = 0, OFF_Q1 = OFF_Q0 + r128(SQ_BYTES);
+constexpr int OFF_V0 = OFF_Q1 + r128(SQ_BYTES), OFF_V1 = OFF_V0 + r128(SV_BYTES);
+constexpr int OFF_N = OFF_V1 + r128(SV_BYTES);
+constexpr int OFF_FI = OFF_N + r128(SN_BYTES);
+constexpr int OFF_FJ = OFF_FI + r128(TY * (TX + 1) * 16);
+constexpr int OFF_BAR = OFF_FJ + r128((TY + 1) * TX * 16);
+constexpr int TMA_SMEM = OFF_BAR + 128 + 128;  // + alignment slack
+}  // namespace
+
+template <int SCHEME, int STAGE, bool EMIT>
+__global__ void __launch_bounds__(NT, AUSM_TMA_MIN_BLOCKS)
+    k_fused_stage_tma(const __grid_constant__ TmaMapsLaunch tm, const float4* __restrict__ Qs,
+                      float4* __restrict__ Qo, const float2* __restrict__ V, const float* __restrict__ dtp,
+                      uint32_t* __restrict__ wave, int* __restrict__ err, const Consts c, const int M, const int N,
+                      const int tilesX, const int numTiles) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  // TMA destinations need 16-byte (we keep 128-byte) alignment of the dynamic region
+  unsigned char* smem = smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u);
+  auto SQ = [&](int b) { return reinterpret_cast<float4(*)[PW]>(smem + OFF_Q0 + b * (OFF_Q1 - OFF_Q0)); };
+  auto SV = [&](int b) { return reinterpret_cast<float2*>(smem + OFF_V0 + b * (OFF_V1 - OFF_V0)); };
+  float4(*SN)[TX] = reinterpret_cast<float4(*)[TX]>(smem + OFF_N);
+  float4(*Fi)[TX + 1] = reinterpret_cast<float4(*)[TX + 1]>(smem + OFF_FI);
+  float4(*Fj)[TX] = reinterpret_cast<float4(*)[TX]>(smem + OFF_FJ);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + OFF_BAR);  // [0],[1] tile buffers, [2] Qn
+
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * NWX + tx;
+  if (tid == 0) {
+    mbar_init(&bars[0], 1);
+    mbar_init(&bars[1], 1);
+    mbar_init(&bars[2], 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+
+  auto issue_tile = [&](int t, int buf) {  // thread 0 only
+    const int i0 = (t % tilesX) * TX, j0 = (t / tilesX) * TY;
+    mbar_expect_tx(&bars[buf], SQ_BYTES + SV_BYTES);
+    tma_load_2d(SQ(buf), &tm.qs, 4 * (i0 - 2), j0 - 2, &bars[buf]);
+    tma_load_2d(SV(buf), &tm.v, 2 * i0, j0, &bars[buf]);
+  };
+
+  const float dt = *dtp;
+  uint32_t wmax = 0u;
+  // thread 0's record of loads in flight: bit q of `pending` for barrier q, bit q of
+  // `phase` the parity of its outstanding phase
+  unsigned pending = 0u, phase = 0u;
+  bool failed = false;
+  int hr, hc;
+  halo_entry(tx, ty, hr, hc);
+
+  if (tid == 0 && blockIdx.x < numTiles) {
+    issue_tile(blockIdx.x, 0);
+    pending |= 1u;
+  }
+  int k = 0;
+  for (int t = blockIdx.x; t < numTiles; t += gridDim.x, ++k) {
+    const int b = k & 1;
+    const int i0 = (t % tilesX) * TX, j0 = (t / tilesX) * TY;
+    if constexpr (STAGE >= 2) {
+      if (tid == 0) {  // Qn of this tile streams in during the face phase
+        fence_proxy_async();
+        mbar_expect_tx(&bars[2], SN_BYTES);
+        tma_load_2d(SN, &tm.qn, 4 * i0, j0, &bars[2]);
+        pending |= 4u;
+      }
+    }
+    // ---- tile k has landed in buffer b ----
+    bool ok = mbar_wait(&bars[b], (k >> 1) & 1);
+    if (__syncthreads_or(!ok)) {
+      failed = true;
+      break;
+    }
+    if (tid == 0) {
+      pending &= ~(1u << b);
+      phase ^= 1u << b;
+    }
+    float4(*P)[PW] = SQ(b);
+    float2* Vs = SV(b);
+    // owned cells and the halo entry: fill seam columns and ghost rows, keep the owned
+    // conserved states, convert to primitives in place
+    auto stage_entry = [&](int pr, int pc) {
+      const int ig = i0 - 2 + pc, j = j0 - 2 + pr;
+      float4 q;
+      if (j >= 0 && j < N) q = (ig >= 0 && ig < M) ? P[pr][pc] : __ldg(&Qs[(size_t)j * M + wrap_i(ig, M)]);
+      else q = tile_cell(Qs, V, c, M, N, wrap_i(ig, M), j);
+      P[pr][pc] = to_prim<true>(q, c.gm1);
+      return q;
+    };
+    const float4 qa = stage_entry(ty + 2, tx + 2);
+    const float4 qb = stage_entry(ty + 10, tx + 2);
+    if (hr >= 0) stage_entry(hr, hc);
+    if (i0 + TX + 1 >= M) {  // vertex columns past the seam
+      for (int r = ty; r <= TY; r += NWY) {
+        const int j = j0 + r;
+        if (j > N) continue;
+        if (i0 + tx >= M) Vs[r * VW_TMA + tx] = __ldg(&V[(size_t)j * M + wrap_i(i0 + tx, M)]);
+        if (tx < 2 && i0 + TX + tx >= M) Vs[r * VW_TMA + TX + tx] = __ldg(&V[(size_t)j * M + wrap_i(i0 + TX + tx, M)]);
+      }
+    }
+    __syncthreads();
+    // ---- prefetch the next tile into the other buffer (free since the last barrier) ----
+    if (tid == 0 && t + (int)gridDim.x < numTiles) {
+      fence_proxy_async();
+      issue_tile(t + gridDim.x, b ^ 1);
+      pending |= 1u << (b ^ 1);
+    }
+    faces_phase<SCHEME, VW_TMA>(P, Vs, Fi, Fj, c, i0, j0, M, N, tx, ty);
+    __syncthreads();
+    if constexpr (STAGE >= 2) {
+      bool okn = mbar_wait(&bars[2], k & 1);
+      if (__syncthreads_or(!okn)) {
+        failed = true;
+        break;
+      }
+      if (tid == 0) {
+        pending &= ~4u;
+        phase ^= 4u;
+      }
+    }
+    auto qn = [&](int h) { return SN[ty + 8 * h][tx]; };
+    wmax = max(wmax, combine_phase<STAGE, EMIT, VW_TMA>(Vs, Fi, Fj, qa, qb, qn, Qo, dt, c, i0, j0, M, N, tx, ty));
+    __syncthreads();  // Fi, Fj, SN and buffer b are free for reuse
+  }
+  if (failed) {
+    if (tid == 0) {
+      atomicExch(err, 1);
+      for (int q = 0; q < 3; q++)  // let copies still in flight land before the CTA exits
+        if (pending & (1u << q)) mbar_wait(&bars[q], (phase >> q) & 1u);
+    }
+    return;
   }
   if constexpr (EMIT) block_max_to(wave, wmax);
 }
@@ -186,32 +359,86 @@ __global__ void __launch_bounds__(NWX* NWY, AUSM_FUSED_MIN_BLOCKS)
 namespace {
 template <int S, int ST, bool E>
 void launch_t(const float4* Qs, const float4* Qn, float4* Qo, const float2* V, const float* dt, uint32_t* wave,
-              const Consts& c, int M, int N, cudaStream_t s) {
-  dim3 grid((M + TX - 1) / TX, (N + TY - 1) / TY);
-  k_fused_stage<S, ST, E><<<grid, dim3(NWX, NWY), 0, s>>>(Qs, Qn, Qo, V, dt, wave, c, M, N);
+              const Consts& c, int M, int N, const TmaMapsLaunch* tm, int* err, cudaStream_t s) {
+  const int tilesX = (M + TX - 1) / TX, tilesY = (N + TY - 1) / TY;
+  if (tm && ST != 0) {
+    static int blocks_per_sm = 0, sms = 0;
+    auto kern = k_fused_stage_tma<S, ST, E>;
+    if (!blocks_per_sm) {
+      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, TMA_SMEM);
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, kern, NT, TMA_SMEM);
+      int dev = 0;
+      cudaGetDevice(&dev);
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+      if (blocks_per_sm < 1) blocks_per_sm = 1;
+    }
+    const int numTiles = tilesX * tilesY;
+    const int grid = std::min(numTiles, blocks_per_sm * sms);
+    kern<<<grid, dim3(NWX, NWY), TMA_SMEM, s>>>(*tm, Qs, Qo, V, dt, wave, err, c, M, N, tilesX, numTiles);
+  } else {
+    k_fused_stage<S, ST, E><<<dim3(tilesX, tilesY), dim3(NWX, NWY), 0, s>>>(Qs, Qn, Qo, V, dt, wave, c, M, N);
+  }
 }
 template <int S>
 void launch_s(int stage, bool emit, const float4* Qs, const float4* Qn, float4* Qo, const float2* V,
-              const float* dt, uint32_t* wave, const Consts& c, int M, int N, cudaStream_t s) {
+              const float* dt, uint32_t* wave, const Consts& c, int M, int N, const TmaMapsLaunch* tm, int* err,
+              cudaStream_t s) {
   switch (stage) {
-    case 0: launch_t<S, 0, false>(Qs, Qn, Qo, V, dt, wave, c, M, N, s); break;
-    case 1: launch_t<S, 1, false>(Qs, Qn, Qo, V, dt, wave, c, M, N, s); break;
-    case 2: launch_t<S, 2, false>(Qs, Qn, Qo, V, dt, wave, c, M, N, s); break;
+    case 0: launch_t<S, 0, false>(Qs, Qn, Qo, V, dt, wave, c, M, N, tm, err, s); break;
+    case 1: launch_t<S, 1, false>(Qs, Qn, Qo, V, dt, wave, c, M, N, tm, err, s); break;
+    case 2: launch_t<S, 2, false>(Qs, Qn, Qo, V, dt, wave, c, M, N, tm, err, s); break;
     default:
-      if (emit) launch_t<S, 3, true>(Qs, Qn, Qo, V, dt, wave, c, M, N, s);
-      else launch_t<S, 3, false>(Qs, Qn, Qo, V, dt, wave, c, M, N, s);
+      if (emit) launch_t<S, 3, true>(Qs, Qn, Qo, V, dt, wave, c, M, N, tm, err, s);
+      else launch_t<S, 3, false>(Qs, Qn, Qo, V, dt, wave, c, M, N, tm, err, s);
   }
 }
 }  // namespace
 
 void launch_fused_stage(int scheme, int stage, bool emit, const float4* Qs, const float4* Qn, float4* Qo,
                         const float2* V, const float* dt, uint32_t* wave, const Consts& c, int M, int N,
-                        cudaStream_t s) {
+                        const TmaMapsLaunch* tm, int* err, cudaStream_t s) {
   switch (scheme) {
-    case 0: launch_s<0>(stage, emit, Qs, Qn, Qo, V, dt, wave, c, M, N, s); break;
-    case 1: launch_s<1>(stage, emit, Qs, Qn, Qo, V, dt, wave, c, M, N, s); break;
-    default: launch_s<2>(stage, emit, Qs, Qn, Qo, V, dt, wave, c, M, N, s); break;
+    case 0: launch_s<0>(stage, emit, Qs, Qn, Qo, V, dt, wave, c, M, N, tm, err, s); break;
+    case 1: launch_s<1>(stage, emit, Qs, Qn, Qo, V, dt, wave, c, M, N, tm, err, s); break;
+    default: launch_s<2>(stage, emit, Qs, Qn, Qo, V, dt, wave, c, M, N, tm, err, s); break;
   }
+}
+
+// Tensor maps of the TMA kernel: state buffers as 2-D float tensors of 4M x N
+// (row pitch 16 M bytes) with the halo box 144 x 20 and the Qn box 128 x 16, vertices
+// as 2M x (N+1) (pitch 8 M bytes, needs M even) with the box 68 x 17.
+bool encode_tma_maps(const float4* const Q[3], const float2* V, int M, int N, TmaMaps* out) {
+  out->ok = false;
+  if (M % 2 != 0) return false;
+  using Encode = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                              const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                              CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+  static Encode encode = nullptr;
+  if (!encode) {
+    cudaDriverEntryPointQueryResult q;
+    void* fn = nullptr;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess || !fn)
+      return false;
+    encode = reinterpret_cast<Encode>(fn);
+  }
+  const cuuint32_t estr[2] = {1, 1};
+  auto enc = [&](CUtensorMap* m, const void* ptr, cuuint64_t w, cuuint64_t h, cuuint64_t pitch, cuuint32_t bw,
+                 cuuint32_t bh) {
+    const cuuint64_t dims[2] = {w, h};
+    const cuuint64_t strides[1] = {pitch};
+    const cuuint32_t box[2] = {bw, bh};
+    return encode(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<void*>(ptr), dims, strides, box, estr,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+  };
+  for (int b = 0; b < 3; b++) {
+    if (!enc(&out->halo[b], Q[b], 4ull * M, N, 16ull * M, 4 * PW, PH)) return false;
+    if (!enc(&out->plain[b], Q[b], 4ull * M, N, 16ull * M, 4 * TX, TY)) return false;
+  }
+  if (!enc(&out->v, V, 2ull * M, N + 1, 8ull * M, 2 * VW_TMA, TY + 1)) return false;
+  out->ok = true;
+  return true;
 }
 
 // Wave speed + max of an interior state with metrics recomputed from the vertices
