@@ -70,6 +70,8 @@ _SIGS = {
     "ausm_forces": [_P, C.POINTER(C.c_double), C.POINTER(C.c_double)],
     "ausm_residual_l2": [_P, C.POINTER(C.c_double)],
     "ausm_field": [_P, C.c_int, C.POINTER(C.c_float)],
+    "ausm_forces_noalloc": [C.c_void_p, C.c_void_p, C.c_int, C.POINTER(AusmParams), C.POINTER(C.c_double),
+                            C.POINTER(C.c_double), C.c_void_p],
     "ausm_stream": [_P, C.POINTER(C.c_void_p)],
     "ausm_synchronize": [_P],
     "ausm_time_steps": [_P, C.c_int, C.c_int, C.POINTER(C.c_float)],

@@ -14,6 +14,11 @@ using namespace ausm;
 
 static thread_local std::string g_err;
 
+namespace ausm {
+// error text for ausm_last_error(NULL) from entry points defined in other files
+void set_thread_error(const std::string& msg) { g_err = msg; }
+}  // namespace ausm
+
 struct ausm_solver {
   int M = 0, N = 0, dev = 0;
   int engine = AUSM_ENGINE_FUSED;

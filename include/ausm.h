@@ -161,6 +161,22 @@ int ausm_residual_l2(ausm_solver* h, double* l2);
 /* Headless field output: M x N floats of AUSM_FIELD_* for the interior. */
 int ausm_field(ausm_solver* h, int kind, float* out);
 
+/* Surface force and wall Cp without allocating anything (no counterpart in the
+ * reference).  For hosts that cannot call cudaMalloc where they need the forces: hosts
+ * that own all device memory through their own pool or arena, hosts that must not
+ * trigger the implicit synchronisation an allocation can cause, and hosts that keep the
+ * state in their own device buffers without a solver handle.  wall_row: device pointer
+ * to the M float4 conserved states of the first interior row (row 1 of the reference
+ * layout); body_xy: device pointer to the M float2 body vertices (vertex row 0);
+ * out6 and cp (M values, may be NULL) are host pointers, filled as by ausm_forces with
+ * the inflow speed mach * sqrt(gamma p / rho) of *p.  stream may be NULL (legacy
+ * default stream); the call waits for it.  Scratch is one fixed array per device of
+ * 3 * 16384 + 2 doubles, so M above 16384 is rejected with AUSM_ERR_INVALID.  The
+ * first call on each device looks up that array's device address, so make it before
+ * any stream capture.  Calls share the array: two calls that overlap on the GPU race. */
+int ausm_forces_noalloc(const void* wall_row, const void* body_xy, int M, const AusmParams* p, double* out6,
+                        double* cp, void* stream);
+
 /* Device stream of the handle (cudaStream_t) and a blocking wait on it. */
 int ausm_stream(ausm_solver* h, void** stream);
 int ausm_synchronize(ausm_solver* h);
