@@ -75,6 +75,17 @@ _SIGS = {
     "ausm_stream": [_P, C.POINTER(C.c_void_p)],
     "ausm_synchronize": [_P],
     "ausm_time_steps": [_P, C.c_int, C.c_int, C.POINTER(C.c_float)],
+    "ausm_batch_create": [C.POINTER(C.c_void_p)],
+    "ausm_batch_destroy": [_P],
+    "ausm_batch_add": [_P, _P],
+    "ausm_batch_remove": [_P, _P],
+    "ausm_batch_size": [_P, C.POINTER(C.c_int)],
+    "ausm_batch_member": [_P, C.c_int, C.POINTER(C.c_void_p)],
+    "ausm_batch_set_graphs": [_P, C.c_int],
+    "ausm_batch_step": [_P, C.c_int, C.POINTER(C.c_float)],
+    "ausm_batch_residual_l2": [_P, C.POINTER(C.c_double)],
+    "ausm_batch_synchronize": [_P],
+    "ausm_batch_time_steps": [_P, C.c_int, C.c_int, C.POINTER(C.c_float)],
 }
 
 
@@ -98,12 +109,15 @@ def lib():
             f.restype = C.c_int
     L.ausm_last_error.argtypes = [_P]
     L.ausm_last_error.restype = C.c_char_p
+    if hasattr(L, "ausm_batch_last_error"):
+        L.ausm_batch_last_error.argtypes = [_P]
+        L.ausm_batch_last_error.restype = C.c_char_p
     _lib = L
     return L
 
 
-def check(rc: int, handle=None):
+def check(rc: int, handle=None, batch=None):
     if rc != OK:
-        msg = lib().ausm_last_error(handle)
+        msg = lib().ausm_batch_last_error(batch) if batch is not None else lib().ausm_last_error(handle)
         raise AusmError(rc, msg.decode() if msg else "")
     return rc

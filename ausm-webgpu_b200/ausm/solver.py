@@ -201,3 +201,91 @@ class Solver:
         ms = C.c_float()
         self._c(lib().ausm_time_steps(self.h, int(n), int(reps), C.byref(ms)))
         return ms.value
+
+
+class Batch:
+    """Many solves stepped together: one persistent kernel launch per RK stage over the
+    tiles of every member (no counterpart in the reference, which steps one grid).
+
+    Members keep their own dt, scheme and parameters; a member's results are the same
+    alone or in any batch.  The n-step sequence is replayed from a CUDA graph."""
+
+    def __init__(self, graphs: bool = True):
+        b = C.c_void_p()
+        check(lib().ausm_batch_create(C.byref(b)))
+        self.b = b
+        self._members: dict[int, Solver] = {}  # handle address -> Solver, kept alive here
+        if not graphs:
+            self.set_graphs(False)
+
+    def close(self):
+        if getattr(self, "b", None):
+            lib().ausm_batch_destroy(self.b)
+            self.b = None
+            self._members = {}
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __len__(self):
+        n = C.c_int()
+        self._c(lib().ausm_batch_size(self.b, C.byref(n)))
+        return n.value
+
+    def _c(self, rc):
+        return check(rc, batch=self.b)
+
+    @property
+    def members(self) -> list[Solver]:
+        """Current members in the library's order (a destroyed solver has left)."""
+        out = []
+        for k in range(len(self)):
+            h = C.c_void_p()
+            self._c(lib().ausm_batch_member(self.b, k, C.byref(h)))
+            out.append(self._members[h.value])
+        return out
+
+    def add(self, s: Solver):
+        self._c(lib().ausm_batch_add(self.b, s.h))
+        self._members[s.h.value] = s
+
+    def remove(self, s: Solver):
+        self._c(lib().ausm_batch_remove(self.b, s.h))
+        self._members.pop(s.h.value, None)
+
+    def set_graphs(self, enable: bool):
+        self._c(lib().ausm_batch_set_graphs(self.b, int(bool(enable))))
+
+    def step(self, n: int = 1, wait: bool = True) -> np.ndarray | None:
+        """n RK3 steps of every member; with wait, returns an (members, 2) array of the
+        dt used and the max wave speed after the steps."""
+        if not wait:
+            self._c(lib().ausm_batch_step(self.b, int(n), None))
+            return None
+        out = np.zeros((len(self), 2), dtype=np.float32)
+        self._c(lib().ausm_batch_step(self.b, int(n), _fp(out) if out.size else None))
+        return out
+
+    def residual_l2(self) -> np.ndarray:
+        out = np.zeros(len(self))
+        if out.size:
+            self._c(lib().ausm_batch_residual_l2(self.b, _dp(out)))
+        return out
+
+    def synchronize(self):
+        self._c(lib().ausm_batch_synchronize(self.b))
+
+    def time_steps(self, n: int, reps: int) -> float:
+        """Device time (ms) of `reps` calls of step(n, wait=False)."""
+        ms = C.c_float()
+        self._c(lib().ausm_batch_time_steps(self.b, int(n), int(reps), C.byref(ms)))
+        return ms.value

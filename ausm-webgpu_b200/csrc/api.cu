@@ -9,6 +9,7 @@
 
 #include "ausm.h"
 #include "ausm_internal.h"
+#include "solver_internal.h"
 
 using namespace ausm;
 
@@ -17,39 +18,43 @@ static thread_local std::string g_err;
 namespace ausm {
 // error text for ausm_last_error(NULL) from entry points defined in other files
 void set_thread_error(const std::string& msg) { g_err = msg; }
+
+// Uniform values as the reference builds them (main.js:779-784, util.js:180-185), in
+// double, rounded to f32; derived constants in f32 in the shaders' operation order.
+void make_consts(ausm_solver* h) {
+  const AusmParams& p = h->p;
+  Consts c{};
+  const float g = (float)p.gamma, inRho = (float)p.in_rho, inP = (float)p.in_pressure;
+  double a = p.aoa_deg * M_PI / 180.0;
+  double u = h->speed_now * std::cos(a), v = h->speed_now * std::sin(a);
+  c.gamma = g; c.inRho = inRho; c.inP = inP;
+  c.gm1 = g - 1.0f;
+  c.gm1inv = 1.0f / (g - 1.0f);
+  c.Kp = (float)p.K_p; c.Ku = (float)p.K_u; c.cfl = (float)p.cfl; c.maxdt = (float)p.maxdt;
+  c.inflow = make_float2((float)u, (float)v);
+  double rhoE = p.in_pressure / (p.gamma - 1.0) + 0.5 * (h->speed_now * h->speed_now) * p.in_rho;
+  c.inState = make_float4(inRho, (float)(u * p.in_rho), (float)(v * p.in_rho), (float)rhoE);
+  c.a2inf = (g * inP) / inRho;
+  c.Vinf2 = c.inflow.x * c.inflow.x + c.inflow.y * c.inflow.y;
+  c.Minf2 = c.Vinf2 / c.a2inf;
+  c.gammaInP = g * inP;
+  c.aStarK = (2.0f * c.gm1) / (g + 1.0f);
+  c.ambE = inP / (g - 1.0f);
+  c.gmgm1 = g / c.gm1;
+  c.muscl = p.muscl;
+  h->c = c;
+}
+
+void ramp_after_steps(ausm_solver* h, int n) {
+  if (h->p.ramp > 0.0 && n > 0) {
+    double target = h->p.mach * std::sqrt(h->p.gamma * h->p.in_pressure / h->p.in_rho);
+    h->speed_now += (target - h->speed_now) / (h->p.ramp / n * 50.0);
+    make_consts(h);
+  }
+}
+
 }  // namespace ausm
 
-struct ausm_solver {
-  int M = 0, N = 0, dev = 0;
-  int engine = AUSM_ENGINE_FUSED;
-  AusmParams p{};
-  double speed_now = 0.0;  // current inflow speed (ramped when p.ramp > 0)
-  Consts c{};
-  cudaStream_t st = nullptr;
-  cudaEvent_t e0 = nullptr, e1 = nullptr;
-  std::vector<double> body, outer;  // M x 2
-  bool has_body = false, has_outer = false, has_grid = false, has_state = false;
-  double stretch = 0.0;
-  float2* V = nullptr;
-  float2* V2 = nullptr;
-  float4* Q[3] = {nullptr, nullptr, nullptr};
-  int cur = 0;
-  float4* S[3] = {nullptr, nullptr, nullptr};
-  float4 *fx = nullptr, *fy = nullptr, *res = nullptr, *flen = nullptr;
-  float* area = nullptr;
-  float4* staging = nullptr;
-  double* cp = nullptr;
-  uint32_t* wave = nullptr;
-  float* dt = nullptr;
-  double* dacc = nullptr;
-  uint32_t* move = nullptr;
-  int* err_flag = nullptr;  // set by a kernel whose bounded wait gave up
-  TmaMaps tma;
-  float* h_dt = nullptr;
-  uint32_t* h_wave = nullptr;
-  double* h_acc = nullptr;
-  std::string err;
-};
 
 namespace {
 
@@ -81,32 +86,6 @@ int use_device(ausm_solver* h) {
 }
 
 double inflow_target(const AusmParams& p) { return p.mach * std::sqrt(p.gamma * p.in_pressure / p.in_rho); }
-
-// Uniform values as the reference builds them (main.js:779-784, util.js:180-185), in
-// double, rounded to f32; derived constants in f32 in the shaders' operation order.
-void make_consts(ausm_solver* h) {
-  const AusmParams& p = h->p;
-  Consts c{};
-  const float g = (float)p.gamma, inRho = (float)p.in_rho, inP = (float)p.in_pressure;
-  double a = p.aoa_deg * M_PI / 180.0;
-  double u = h->speed_now * std::cos(a), v = h->speed_now * std::sin(a);
-  c.gamma = g; c.inRho = inRho; c.inP = inP;
-  c.gm1 = g - 1.0f;
-  c.gm1inv = 1.0f / (g - 1.0f);
-  c.Kp = (float)p.K_p; c.Ku = (float)p.K_u; c.cfl = (float)p.cfl; c.maxdt = (float)p.maxdt;
-  c.inflow = make_float2((float)u, (float)v);
-  double rhoE = p.in_pressure / (p.gamma - 1.0) + 0.5 * (h->speed_now * h->speed_now) * p.in_rho;
-  c.inState = make_float4(inRho, (float)(u * p.in_rho), (float)(v * p.in_rho), (float)rhoE);
-  c.a2inf = (g * inP) / inRho;
-  c.Vinf2 = c.inflow.x * c.inflow.x + c.inflow.y * c.inflow.y;
-  c.Minf2 = c.Vinf2 / c.a2inf;
-  c.gammaInP = g * inP;
-  c.aStarK = (2.0f * c.gm1) / (g + 1.0f);
-  c.ambE = inP / (g - 1.0f);
-  c.gmgm1 = g / c.gm1;
-  c.muscl = p.muscl;
-  h->c = c;
-}
 
 int ensure_reference_buffers(ausm_solver* h) {
   if (h->S[0]) return AUSM_OK;
@@ -225,6 +204,7 @@ int ausm_device_count(int* count) {
 
 int ausm_destroy(ausm_solver* h) {
   if (!h) return AUSM_OK;
+  if (h->batch) ausm_batch_remove(h->batch, h);
   cudaSetDevice(h->dev);
   if (h->st) cudaStreamSynchronize(h->st);
   void* dptrs[] = {h->V, h->V2, h->Q[0], h->Q[1], h->Q[2], h->S[0], h->S[1], h->S[2], h->fx, h->fy, h->res,
@@ -236,7 +216,7 @@ int ausm_destroy(ausm_solver* h) {
   if (h->h_acc) cudaFreeHost(h->h_acc);
   if (h->e0) cudaEventDestroy(h->e0);
   if (h->e1) cudaEventDestroy(h->e1);
-  if (h->st) cudaStreamDestroy(h->st);
+  if (h->own_st) cudaStreamDestroy(h->own_st);
   delete h;
   return AUSM_OK;
 }
@@ -269,6 +249,7 @@ int ausm_create(int M, int N, ausm_solver** out) {
     }                                 \
   } while (0)
   TRY(cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking));
+  h->own_st = h->st;
   TRY(cudaEventCreate(&h->e0));
   TRY(cudaEventCreate(&h->e1));
   size_t n = (size_t)M * N;
@@ -312,6 +293,7 @@ int ausm_set_engine(ausm_solver* h, int engine) {
   NEED(h, h, AUSM_ERR_INVALID, "null handle");
   NEED(h, engine == AUSM_ENGINE_FUSED || engine == AUSM_ENGINE_REFERENCE, AUSM_ERR_INVALID, "unknown engine");
   if (engine == h->engine) return AUSM_OK;
+  NEED(h, !h->batch, AUSM_ERR_STATE, "a batch member stays on the fused engine; remove it from the batch first");
   int rc = use_device(h);
   if (rc) return rc;
   if (engine == AUSM_ENGINE_REFERENCE) {
@@ -638,11 +620,7 @@ int ausm_step(ausm_solver* h, int n, float* dt_out) {
     }
   }
   CHECK_LAUNCH(h);
-  if (h->p.ramp > 0.0 && n > 0) {  // main.js:779
-    double target = inflow_target(h->p);
-    h->speed_now += (target - h->speed_now) / (h->p.ramp / n * 50.0);
-    make_consts(h);
-  }
+  ramp_after_steps(h, n);
   if (dt_out) {
     CU(h, cudaMemcpyAsync(h->h_dt, h->dt, sizeof(float), cudaMemcpyDeviceToHost, s));
     CU(h, cudaMemcpyAsync(h->h_wave, h->wave, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));

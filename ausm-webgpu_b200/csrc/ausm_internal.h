@@ -69,6 +69,32 @@ void launch_fused_stage(int scheme, int stage, bool emit, const float4* Qs, cons
 void launch_wave_interior(const float4* Q, const float2* V, float gamma, int M, int N, uint32_t* wave,
                           cudaStream_t s);
 
+// ---- batched engine (kernels_batch.cu) ----
+// One solve of a batch as the device sees it.  Its tiles are work items
+// tile0 .. tile0 + tiles_x * tiles_y - 1 of the batch; cur is the index of the buffer
+// holding the current state (the RK3 buffers rotate by one per step).
+struct BatchSolve {
+  float4* Q[3];
+  const float2* V;
+  float* dt;
+  uint32_t* wave;
+  Consts c;
+  int M, N, scheme, tiles_x, tile0, cur;
+};
+// All launches go to stream s.  rot: steps already taken since the descriptors' cur.
+// Stage 0 writes the residual dQ/dt of the current state into the solve's next buffer.
+// A stage launch covers one scheme group: descriptors [s_lo, s_hi), items [t_lo, t_hi).
+void launch_batch_dt(BatchSolve* d, int nsolves, cudaStream_t s);
+void launch_batch_stage(int scheme, int stage, bool emit, const BatchSolve* d, int s_lo, int s_hi, int t_lo,
+                        int t_hi, int rot, cudaStream_t s);
+void launch_batch_advance(BatchSolve* d, int nsolves, int steps, cudaStream_t s);
+// out[2 s] = dt, out[2 s + 1] = max wave speed of solve s
+void launch_batch_gather(const BatchSolve* d, int nsolves, float* out, cudaStream_t s);
+// l2[s] = sqrt(mean over solve s's cells of (d rho / dt)^2), from the stage-0 residual;
+// part holds one double per tile.  Summation order depends only on the solve's own grid.
+void launch_batch_residual_norm(const BatchSolve* d, int nsolves, int total_tiles, double* part, double* l2,
+                                cudaStream_t s);
+
 // ---- reference-shaped engine (kernels_reference.cu, built with -fmad=false) ----
 // States use the reference layout [N+3][M] (row 0 wall ghost).
 void launch_ref_metrics(const float2* V, float* area, float4* flen, int M, int N, cudaStream_t s);

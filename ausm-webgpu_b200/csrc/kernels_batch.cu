@@ -1,0 +1,192 @@
+// Batched stage kernel: one launch per RK stage and scheme advances every solve of that
+// scheme in a batch of independent O-grids of any sizes (stage 0: residual only).  The
+// work list is the concatenation of all solves' 32 x 16 tiles, grouped by scheme; each
+// CTA takes one work item, finds its solve by binary search over the solves'
+// first-tile offsets, and runs the same tile compute as the single-solve kernel
+// (stage_tile.cuh) with that solve's buffers, constants and dt.  The scheme is a
+// template parameter: a run-time scheme switch inside one kernel holds all three flux
+// variants' registers at once and spills at the 64-register budget of 4 CTAs per SM.
+// One CTA per item rather than a persistent grid-stride loop: the hardware block
+// scheduler hands out items dynamically, and on B200 the persistent form ran 8% slower.
+// Each solve's dt comes from its own max wave speed, so a solve's arithmetic is the
+// same alone or in any batch.  The buffer rotation lives in the descriptors (cur,
+// advanced on the device after a step sequence), so one captured CUDA graph of n steps
+// can be replayed for any number of rounds.
+#include <algorithm>
+
+#include "stage_tile.cuh"
+
+namespace ausm {
+using namespace tile;
+
+#ifndef AUSM_BATCH_MIN_BLOCKS
+#define AUSM_BATCH_MIN_BLOCKS 4
+#endif
+
+// solve owning work item `item` among descriptors [lo, hi): the last whose first tile
+// is <= item
+__device__ __forceinline__ int solve_of(const BatchSolve* __restrict__ solves, int lo, int hi, int item) {
+  hi -= 1;
+  while (lo < hi) {
+    int mid = (lo + hi + 1) >> 1;
+    if (solves[mid].tile0 <= item) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+// One CTA per work item of one scheme group: item t0 + blockIdx.x, its solve among
+// descriptors [s_lo, s_hi).
+template <int SCHEME, int STAGE, bool EMIT>
+__global__ void __launch_bounds__(NT, AUSM_BATCH_MIN_BLOCKS)
+    k_batch_stage(const BatchSolve* __restrict__ solves, const int s_lo, const int s_hi, const int t0, const int rot) {
+  __shared__ float4 P[PH][PW];
+  __shared__ float2 Vs[(TY + 1) * (TX + 1)];
+  __shared__ float4 Fi[TY][TX + 1];
+  __shared__ float4 Fj[TY + 1][TX];
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int item = t0 + blockIdx.x;
+  const BatchSolve& d = solves[solve_of(solves, s_lo, s_hi, item)];
+  const Consts c = d.c;
+  const int M = d.M, N = d.N;
+  const int local = item - d.tile0;
+  const int i0 = (local % d.tiles_x) * TX, j0 = (local / d.tiles_x) * TY;
+  const int a = (d.cur + rot) % 3, b = (a + 1) % 3, c3 = (a + 2) % 3;
+  const float4* Qs = d.Q[STAGE <= 1 ? a : (STAGE == 2 ? b : c3)];
+  const float4* Qn = d.Q[a];
+  float4* Qo = d.Q[STAGE == 2 ? c3 : b];
+  const float2* V = d.V;
+
+  const int ic = wrap_i(i0 + tx, M);
+  const float4 qa = tile_cell(Qs, V, c, M, N, ic, j0 + ty);
+  const float4 qb = tile_cell(Qs, V, c, M, N, ic, j0 + ty + 8);
+  int hr, hc;
+  halo_entry(tx, ty, hr, hc);
+  float4 qh = make_float4(1.0f, 0.0f, 0.0f, 1.0f);
+  if (hr >= 0) qh = tile_cell(Qs, V, c, M, N, wrap_i(i0 - 2 + hc, M), j0 - 2 + hr);
+  for (int r = ty; r <= TY; r += NWY) {
+    int j = j0 + r;
+    if (j <= N) {
+      Vs[r * (TX + 1) + tx] = __ldg(&V[(size_t)j * M + ic]);
+      if (tx == 0) Vs[r * (TX + 1) + TX] = __ldg(&V[(size_t)j * M + wrap_i(i0 + TX, M)]);
+    }
+  }
+  P[ty + 2][tx + 2] = to_prim<true>(qa, c.gm1);
+  P[ty + 10][tx + 2] = to_prim<true>(qb, c.gm1);
+  if (hr >= 0) P[hr][hc] = to_prim<true>(qh, c.gm1);
+  __syncthreads();
+
+  faces_phase<SCHEME, TX + 1>(P, Vs, Fi, Fj, c, i0, j0, M, N, tx, ty);
+  __syncthreads();
+
+  auto qn = [&](int h) { return __ldg(&Qn[(size_t)(j0 + ty + 8 * h) * M + i0 + tx]); };
+  uint32_t w = combine_phase<STAGE, EMIT, TX + 1>(Vs, Fi, Fj, qa, qb, qn, Qo, *d.dt, c, i0, j0, M, N, tx, ty);
+  if constexpr (EMIT) {
+    w = __reduce_max_sync(0xffffffffu, w);
+    if (tx == 0) atomicMax(d.wave, w);
+  }
+}
+
+// dt = min(maxdt, cfl / max wave speed) per solve (ausm.js:457), then the wave-speed
+// accumulator is cleared for the step sequence's last stage 3.
+__global__ void k_batch_dt(BatchSolve* __restrict__ solves, int n) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  BatchSolve& d = solves[s];
+  d.dt[0] = fminf(d.c.maxdt, d.c.cfl / __uint_as_float(d.wave[0]));
+  d.wave[0] = 0u;
+}
+__global__ void k_batch_advance(BatchSolve* __restrict__ solves, int n, int steps) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s < n) solves[s].cur = (solves[s].cur + steps) % 3;
+}
+
+__global__ void k_batch_gather(const BatchSolve* __restrict__ solves, int n, float* __restrict__ out) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  out[2 * s] = solves[s].dt[0];
+  out[2 * s + 1] = __uint_as_float(solves[s].wave[0]);
+}
+
+// One CTA per tile: sum of (d rho / dt)^2 over the tile's cells of the stage-0 output,
+// in a fixed order (strided per-thread sums, then a shared-memory tree).
+__global__ void __launch_bounds__(256) k_batch_tile_sumsq(const BatchSolve* __restrict__ solves, int nsolves,
+                                                          double* __restrict__ part) {
+  const int item = blockIdx.x;
+  const BatchSolve& d = solves[solve_of(solves, 0, nsolves, item)];
+  const int local = item - d.tile0;
+  const int i0 = (local % d.tiles_x) * TX, j0 = (local / d.tiles_x) * TY;
+  const float4* R = d.Q[(d.cur + 1) % 3];
+  double acc = 0.0;
+  for (int k = threadIdx.x; k < TX * TY; k += 256) {
+    int i = i0 + (k % TX), j = j0 + k / TX;
+    if (i < d.M && j < d.N) {
+      double r = R[(size_t)j * d.M + i].x;
+      acc += r * r;
+    }
+  }
+  __shared__ double sh[256];
+  sh[threadIdx.x] = acc;
+  __syncthreads();
+  for (int w = 128; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) part[item] = sh[0];
+}
+
+// One warp per solve: lane-strided sums over the solve's tiles, then a fixed butterfly.
+__global__ void k_batch_norm(const BatchSolve* __restrict__ solves, int nsolves, const double* __restrict__ part,
+                             double* __restrict__ l2) {
+  const int s = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+  if (s >= nsolves) return;
+  const BatchSolve& d = solves[s];
+  const int ntiles = d.tiles_x * ((d.N + TY - 1) / TY);
+  double acc = 0.0;
+  for (int t = lane; t < ntiles; t += 32) acc += part[d.tile0 + t];
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if (lane == 0) l2[s] = sqrt(acc / ((double)d.M * d.N));
+}
+
+void launch_batch_gather(const BatchSolve* d, int nsolves, float* out, cudaStream_t s) {
+  k_batch_gather<<<(nsolves + 127) / 128, 128, 0, s>>>(d, nsolves, out);
+}
+void launch_batch_residual_norm(const BatchSolve* d, int nsolves, int total_tiles, double* part, double* l2,
+                                cudaStream_t s) {
+  if (total_tiles <= 0) return;
+  k_batch_tile_sumsq<<<total_tiles, 256, 0, s>>>(d, nsolves, part);
+  k_batch_norm<<<(nsolves + 3) / 4, 128, 0, s>>>(d, nsolves, part, l2);
+}
+
+void launch_batch_dt(BatchSolve* d, int nsolves, cudaStream_t s) {
+  k_batch_dt<<<(nsolves + 127) / 128, 128, 0, s>>>(d, nsolves);
+}
+void launch_batch_advance(BatchSolve* d, int nsolves, int steps, cudaStream_t s) {
+  k_batch_advance<<<(nsolves + 127) / 128, 128, 0, s>>>(d, nsolves, steps);
+}
+
+namespace {
+template <int SC, int ST, bool E>
+void launch_b(const BatchSolve* d, int s_lo, int s_hi, int t_lo, int t_hi, int rot, cudaStream_t s) {
+  k_batch_stage<SC, ST, E><<<t_hi - t_lo, dim3(NWX, NWY), 0, s>>>(d, s_lo, s_hi, t_lo, rot);
+}
+template <int SC>
+void launch_scheme(int stage, bool emit, const BatchSolve* d, int s_lo, int s_hi, int t_lo, int t_hi, int rot,
+                   cudaStream_t s) {
+  if (stage == 0) launch_b<SC, 0, false>(d, s_lo, s_hi, t_lo, t_hi, rot, s);
+  else if (stage == 1) launch_b<SC, 1, false>(d, s_lo, s_hi, t_lo, t_hi, rot, s);
+  else if (stage == 2) launch_b<SC, 2, false>(d, s_lo, s_hi, t_lo, t_hi, rot, s);
+  else if (emit) launch_b<SC, 3, true>(d, s_lo, s_hi, t_lo, t_hi, rot, s);
+  else launch_b<SC, 3, false>(d, s_lo, s_hi, t_lo, t_hi, rot, s);
+}
+}  // namespace
+
+void launch_batch_stage(int scheme, int stage, bool emit, const BatchSolve* d, int s_lo, int s_hi, int t_lo,
+                        int t_hi, int rot, cudaStream_t s) {
+  if (t_hi <= t_lo) return;
+  if (scheme == 0) launch_scheme<0>(stage, emit, d, s_lo, s_hi, t_lo, t_hi, rot, s);
+  else if (scheme == 1) launch_scheme<1>(stage, emit, d, s_lo, s_hi, t_lo, t_hi, rot, s);
+  else launch_scheme<2>(stage, emit, d, s_lo, s_hi, t_lo, t_hi, rot, s);
+}
+
+}  // namespace ausm

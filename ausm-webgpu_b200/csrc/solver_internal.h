@@ -1,0 +1,49 @@
+// Host-side state of a solver handle, shared by the C-ABI files (api.cu, batch.cu).
+#pragma once
+#include <string>
+#include <vector>
+
+#include "ausm.h"
+#include "ausm_internal.h"
+
+struct ausm_solver {
+  int M = 0, N = 0, dev = 0;
+  int engine = AUSM_ENGINE_FUSED;
+  AusmParams p{};
+  double speed_now = 0.0;  // current inflow speed (ramped when p.ramp > 0)
+  ausm::Consts c{};
+  cudaStream_t st = nullptr;      // the stream calls run on (the batch's while a member)
+  cudaStream_t own_st = nullptr;  // the handle's own stream
+  ausm_batch* batch = nullptr;    // batch this solver belongs to, if any
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  std::vector<double> body, outer;  // M x 2
+  bool has_body = false, has_outer = false, has_grid = false, has_state = false;
+  double stretch = 0.0;
+  float2* V = nullptr;
+  float2* V2 = nullptr;
+  float4* Q[3] = {nullptr, nullptr, nullptr};
+  int cur = 0;
+  float4* S[3] = {nullptr, nullptr, nullptr};
+  float4 *fx = nullptr, *fy = nullptr, *res = nullptr, *flen = nullptr;
+  float* area = nullptr;
+  float4* staging = nullptr;
+  double* cp = nullptr;
+  uint32_t* wave = nullptr;
+  float* dt = nullptr;
+  double* dacc = nullptr;
+  uint32_t* move = nullptr;
+  int* err_flag = nullptr;  // set by a kernel whose bounded wait gave up
+  ausm::TmaMaps tma;
+  float* h_dt = nullptr;
+  uint32_t* h_wave = nullptr;
+  double* h_acc = nullptr;
+  std::string err;
+};
+
+namespace ausm {
+// Reference-order f32 uniforms of h's parameters and current inflow speed (api.cu).
+void make_consts(ausm_solver* h);
+// Inflow speed update of a ramped start after n steps (main.js:779), api.cu.
+void ramp_after_steps(ausm_solver* h, int n);
+void set_thread_error(const std::string& msg);
+}  // namespace ausm

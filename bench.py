@@ -43,6 +43,14 @@ WORKLOAD = dict(name="naca0024_4096x3072_m6_aoa4_slau2", naca=24, M=4096, N=3072
 ALG_BYTES_PER_CELL_STEP = 152  # 3 stages x (16 in + 16 out) + 2 x 16 Qn + 3 x 8 vertex
 METRIC = "Mcell-updates/s per RK3 step"
 
+# 64 independent O-grids, cells log-uniform from 128x96 to 1024x768 (aspect 4:3), random
+# NACA 4-digit bodies (camber 0-6 %, position 0.2-0.6, thickness 8-18 %), Mach U[0.1, 3],
+# AoA U[-4, 8] deg, scheme uniform over SLAU2 / SLAU / AUSM+-up, 5000 RK3 steps each from
+# a uniform freestream start, CFL 0.5; seeded.
+BATCH = dict(name="batch64_uneven_128x96-1024x768_5000steps", count=64, seed=20261203, cells_lo=128 * 96,
+             cells_hi=1024 * 768, steps=5000, chunk=100, far_chords=20.0, first_spacing=1e-3, cfl=0.5,
+             grid_iters=200)
+
 
 def env_rank():
     return int(os.environ.get("RANK", 0)), int(os.environ.get("LOCAL_RANK", 0)), int(os.environ.get("WORLD_SIZE", 1))
@@ -138,6 +146,89 @@ def build_solver(ausm, wl, engine="fused", M=None, N=None):
                  K_u=0.75, cfl=wl["cfl"], maxdt=math.inf, muscl=1, scheme=wl["scheme"], ramp=0.0)
     s.prepare_state("freestream")
     return s
+
+
+def batch_specs(cfg):
+    import numpy as np
+    rng = np.random.default_rng(cfg["seed"])
+    out = []
+    lo, hi = math.log(cfg["cells_lo"]), math.log(cfg["cells_hi"])
+    for _ in range(cfg["count"]):
+        cells = math.exp(rng.uniform(lo, hi))
+        M = max(16, int(round(math.sqrt(cells * 4.0 / 3.0) / 2)) * 2)
+        N = max(12, int(round(M * 0.75)))
+        m, pos, t = int(rng.integers(0, 7)), int(rng.integers(2, 7)), int(rng.integers(8, 19))
+        out.append(dict(M=M, N=N, naca=m * 1000 + (pos * 100 if m else 0) + t, mach=float(rng.uniform(0.1, 3.0)),
+                        aoa=float(rng.uniform(-4.0, 8.0)), scheme=int(rng.integers(0, 3))))
+    return out
+
+
+def build_spec_solver(ausm, sp, cfg):
+    s = ausm.Solver(sp["M"], sp["N"])
+    s.set_body_naca4(sp["naca"], 0.5, 0.0)
+    s.set_outer_circle(cfg["far_chords"])
+    s.set_radial_stretch(cfg["first_spacing"])
+    s.generate_grid(cfg["grid_iters"], "multicolor")
+    s.set_params(gamma=1.4, in_rho=1.0, in_pressure=1.0 / 1.4, mach=sp["mach"], aoa_deg=sp["aoa"], K_p=0.0,
+                 K_u=0.75, cfl=cfg["cfl"], maxdt=math.inf, muscl=1, scheme=sp["scheme"], ramp=0.0)
+    s.prepare_state("freestream")
+    return s
+
+
+def run_batched(ausm, cfg, warmup):
+    """Config: BATCH.  The same 64 solves (a) in one batch (one persistent launch per
+    RK stage over all their tiles, graph-replayed chunks of cfg['chunk'] steps) and (b)
+    by the plain path, one solve after another, each ausm_step(chunk) call launching its
+    own three stage kernels per step.  dt is recomputed every chunk steps in both.  Both
+    start from the freestream state; solves/s = 64 / elapsed.  The surface Cp of both
+    runs is compared at the end."""
+    import numpy as np
+    specs = batch_specs(cfg)
+    sols = [build_spec_solver(ausm, sp, cfg) for sp in specs]
+    cells = sum(sp["M"] * sp["N"] for sp in specs)
+    steps, chunk = cfg["steps"], cfg["chunk"]
+    b = ausm.Batch()
+    for s in sols:
+        b.add(s)
+    for _ in range(warmup):
+        b.step(chunk, wait=False)
+    for s in sols:
+        s.prepare_state("freestream")
+    b.synchronize()
+    t0 = time.perf_counter()
+    ms = b.time_steps(chunk, steps // chunk)
+    wall_b = time.perf_counter() - t0
+    cp_b = [s.forces(with_cp=True)["Cp"] for s in sols]
+    diverged = int(sum(1 for s in sols if not math.isfinite(s.max_wave_speed())))
+    for s in list(b.members):
+        b.remove(s)
+    b.close()
+    for s in sols:  # plain path warm-up, then the same start
+        s.step(1)
+        s.prepare_state("freestream")
+        s.synchronize()
+    t0 = time.perf_counter()
+    for s in sols:  # dt held over `chunk` steps, as in the batch
+        for _ in range(steps // chunk):
+            s.step(chunk, wait=False)
+        s.synchronize()
+    wall_p = time.perf_counter() - t0
+    cp_p = [s.forces(with_cp=True)["Cp"] for s in sols]
+    err = 0.0
+    for a, c in zip(cp_b, cp_p):
+        if np.all(np.isfinite(a)) and np.all(np.isfinite(c)):
+            err = max(err, float(np.abs(a - c).max() / max(np.abs(c).max(), 1e-30)))
+    for s in sols:
+        s.close()
+    n = len(specs)
+    return {"metric": "batched solves/s", "value": n / (ms * 1e-3), "unit": "solves/s",
+            "workload": cfg["name"], "solves": n, "cells_total": cells, "steps_per_solve": steps,
+            "device_ms": ms, "wall_s": wall_b, "solves_per_s_wall": n / wall_b,
+            "plain_one_launch_per_solve": {"wall_s": wall_p, "solves_per_s": n / wall_p},
+            "speedup_vs_plain": wall_p / wall_b, "cp_max_rel_diff_vs_plain": err, "diverged": diverged,
+            "mcell_updates_per_s": cells * steps / (ms * 1e-3) / 1e6,
+            "gpu_launches": (3 * chunk + 3) * (steps // chunk),
+            "sizes": f"{min(sp['M'] * sp['N'] for sp in specs)}..{max(sp['M'] * sp['N'] for sp in specs)} cells"}
 
 
 def cpu_reference_sample(wl, vertices=None, target_s=20.0, K=1):
@@ -236,6 +327,10 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--small", action="store_true", help="512x384 grid (profiling and quick checks)")
+    ap.add_argument("--mode", default="step", choices=["step", "batch"],
+                    help="step: the 4096x3072 step (headline line, with the batched measurement "
+                         "attached); batch: the batched measurement alone")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched measurement in --mode step")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -251,6 +346,11 @@ def main():
     import numpy as np
     import ausm
     ausm.set_device(local_rank)
+    if args.mode == "batch":
+        res = run_batched(ausm, BATCH, args.warmup)
+        if rank == 0:
+            print(json.dumps(res))
+        return 0
     wl = dict(WORKLOAD)
     if args.small:
         wl.update(M=512, N=384, name="naca0024_512x384_m6_aoa4_slau2")
@@ -321,6 +421,12 @@ def main():
         except Exception as e:  # the baseline is reported, never required
             cpu = {"value": None, "unit": "Mcell-updates/s", "cores": None, "kind": None, "sample": f"failed: {e}"}
 
+    batched = None
+    if world == 1 and not args.no_batch and not args.small:
+        s.close()
+        s = None
+        batched = run_batched(ausm, BATCH, args.warmup)
+
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "Mcell-updates/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -329,9 +435,10 @@ def main():
                            "parallelism": f"replicas{world}", "l2": "inputs larger than L2 (201 MB state)",
                            "wall_s": wall},
                 "gpu_launches": (4 if args.engine == "fused" else 17) * args.steps, "clocks": clocks, "roofline": roofline, "cpu_baseline": cpu,
-                "e2e": e2e}
+                "e2e": e2e, "batched": batched}
         print(json.dumps(line))
-    s.close()
+    if s is not None:
+        s.close()
     if dist:
         dist.barrier()
         dist.destroy_process_group()

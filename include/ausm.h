@@ -184,6 +184,42 @@ int ausm_synchronize(ausm_solver* h);
  * on the handle's stream; ms_out gets the elapsed device time of all of them. */
 int ausm_time_steps(ausm_solver* h, int n, int reps, float* ms_out);
 
+/* ---- batches: many solves advanced together (no counterpart in the reference) ----
+ * The reference steps one grid per page.  A batch steps any number of independent
+ * fused-engine solvers of any grid sizes and schemes with ONE persistent kernel launch
+ * per RK stage: the work list is every member's 32 x 16 cell tiles end to end.  Each
+ * member keeps its own dt (from its own max wave speed, held over the n steps as
+ * ausm_step does), so a member's results are the same alone or in any batch.  While a
+ * solver is a member, its calls run on the batch's stream (ausm_stream returns it) and
+ * its engine cannot change; destroying a member removes it first.  A member may belong
+ * to one batch.  With graphs on (the default) the n-step sequence is captured once per
+ * (membership, n) as a CUDA graph and replayed. */
+typedef struct ausm_batch ausm_batch;
+/* New empty batch on the current device. */
+int ausm_batch_create(ausm_batch** out);
+int ausm_batch_destroy(ausm_batch* b);
+const char* ausm_batch_last_error(const ausm_batch* b);
+/* Add a solver that has a grid and a state (fused engine, same device). */
+int ausm_batch_add(ausm_batch* b, ausm_solver* h);
+/* Remove a member; AUSM_ERR_NOT_FOUND if h is not one. */
+int ausm_batch_remove(ausm_batch* b, ausm_solver* h);
+int ausm_batch_size(const ausm_batch* b, int* n);
+/* Member k (in order of addition, removals close the gap). */
+int ausm_batch_member(const ausm_batch* b, int k, ausm_solver** h);
+int ausm_batch_set_graphs(ausm_batch* b, int enable);
+/* n RK3 steps of every member.  dt_wave (2 floats per member, may be NULL): the dt used
+ * and the max wave speed after the steps; with it the call waits for the GPU and
+ * returns AUSM_ERR_DIVERGED (after filling dt_wave) when a member's wave speed is not
+ * finite.  Without it the call only enqueues the work. */
+int ausm_batch_step(ausm_batch* b, int n, float* dt_wave);
+/* Density-residual L2 norm of every member's current state (as ausm_residual_l2), one
+ * double per member; waits for the GPU. */
+int ausm_batch_residual_l2(ausm_batch* b, double* l2);
+int ausm_batch_synchronize(ausm_batch* b);
+/* Device-timed loop: `reps` calls of ausm_batch_step(b, n, NULL); ms_out gets the
+ * elapsed device time of all of them. */
+int ausm_batch_time_steps(ausm_batch* b, int n, int reps, float* ms_out);
+
 #ifdef __cplusplus
 }
 #endif
