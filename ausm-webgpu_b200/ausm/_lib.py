@@ -39,6 +39,31 @@ class AusmParams(C.Structure):
                 ("ramp", C.c_double)]
 
 
+class AusmRequest(C.Structure):
+    _fields_ = [("M", C.c_int), ("N", C.c_int), ("naca4", C.c_int), ("closed_te", C.c_int),
+                ("body_xy", C.POINTER(C.c_double)), ("chord", C.c_double), ("far_radius", C.c_double),
+                ("first_spacing", C.c_double), ("grid_iters", C.c_int), ("init_mode", C.c_int),
+                ("params", AusmParams), ("residual_drop", C.c_double), ("max_steps", C.c_int)]
+
+
+class AusmResult(C.Structure):
+    _fields_ = [("id", C.c_int64), ("state", C.c_int), ("stop", C.c_int), ("M", C.c_int), ("N", C.c_int),
+                ("steps", C.c_int), ("l2_first", C.c_double), ("l2_last", C.c_double),
+                ("forces", C.c_double * 6), ("queue_ms", C.c_double), ("run_ms", C.c_double),
+                ("latency_ms", C.c_double)]
+
+
+class AusmServerStats(C.Structure):
+    _fields_ = [("submitted", C.c_int64), ("rejected", C.c_int64), ("admitted", C.c_int64),
+                ("finished", C.c_int64), ("failed", C.c_int64), ("rounds", C.c_int64), ("pending", C.c_int),
+                ("active", C.c_int), ("bytes_in_use", C.c_double), ("peak_bytes", C.c_double),
+                ("cell_updates", C.c_double)]
+
+
+REQ_DONE, REQ_QUEUED, REQ_RUNNING = 0, 1, 2
+STOP_CONVERGED, STOP_MAX_STEPS, STOP_DIVERGED = 1, 2, 3
+SERVE_PLAIN, SERVE_NO_GRAPH = 1, 2
+
 _lib = None
 
 _P = C.c_void_p
@@ -86,6 +111,16 @@ _SIGS = {
     "ausm_batch_residual_l2": [_P, C.POINTER(C.c_double)],
     "ausm_batch_synchronize": [_P],
     "ausm_batch_time_steps": [_P, C.c_int, C.c_int, C.POINTER(C.c_float)],
+    "ausm_server_create": [C.c_double, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_void_p)],
+    "ausm_server_destroy": [_P],
+    "ausm_request_bytes": [C.POINTER(AusmRequest), C.POINTER(C.c_double)],
+    "ausm_server_submit": [_P, C.POINTER(AusmRequest), C.POINTER(C.c_int64)],
+    "ausm_server_pump": [_P, C.POINTER(C.c_int)],
+    "ausm_server_start": [_P],
+    "ausm_server_stop": [_P],
+    "ausm_server_poll": [_P, C.c_int64, C.POINTER(AusmResult), C.POINTER(C.c_double)],
+    "ausm_server_drain": [_P, C.c_double],
+    "ausm_server_stats": [_P, C.POINTER(AusmServerStats)],
 }
 
 
@@ -109,15 +144,21 @@ def lib():
             f.restype = C.c_int
     L.ausm_last_error.argtypes = [_P]
     L.ausm_last_error.restype = C.c_char_p
-    if hasattr(L, "ausm_batch_last_error"):
-        L.ausm_batch_last_error.argtypes = [_P]
-        L.ausm_batch_last_error.restype = C.c_char_p
+    for name in ("ausm_batch_last_error", "ausm_server_last_error"):
+        if hasattr(L, name):
+            getattr(L, name).argtypes = [_P]
+            getattr(L, name).restype = C.c_char_p
     _lib = L
     return L
 
 
-def check(rc: int, handle=None, batch=None):
+def check(rc: int, handle=None, batch=None, server=None):
     if rc != OK:
-        msg = lib().ausm_batch_last_error(batch) if batch is not None else lib().ausm_last_error(handle)
+        if server is not None:
+            msg = lib().ausm_server_last_error(server)
+        elif batch is not None:
+            msg = lib().ausm_batch_last_error(batch)
+        else:
+            msg = lib().ausm_last_error(handle)
         raise AusmError(rc, msg.decode() if msg else "")
     return rc

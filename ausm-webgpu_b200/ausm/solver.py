@@ -289,3 +289,107 @@ class Batch:
         ms = C.c_float()
         self._c(lib().ausm_batch_time_steps(self.b, int(n), int(reps), C.byref(ms)))
         return ms.value
+
+
+def make_request(M: int, N: int, naca4: int = 12, body_xy=None, chord: float = 1.0, far_radius: float = 20.0,
+                 first_spacing: float = 1e-3, grid_iters: int = 200, init: str = "freestream",
+                 residual_drop: float = 4.0, max_steps: int = 50000, closed_te: bool = True, **flow):
+    """An AusmRequest; flow keywords are AusmParams fields (mach, aoa_deg, scheme, cfl, ...)
+    over the library defaults with cfl 0.5 and no dt cap.  The returned request keeps
+    a reference to the body array it points at."""
+    p = default_params()
+    p.cfl, p.maxdt = 0.5, float("inf")
+    for k, v in flow.items():
+        if k == "scheme" and isinstance(v, str):
+            v = _lib.SCHEMES[v]
+        if not hasattr(p, k):
+            raise AusmError(_lib.ERR_INVALID, f"unknown parameter {k}")
+        setattr(p, k, v)
+    r = _lib.AusmRequest()
+    r.M, r.N, r.naca4, r.closed_te = int(M), int(N), int(naca4), int(bool(closed_te))
+    if body_xy is not None:
+        body = np.ascontiguousarray(body_xy, dtype=np.float64).reshape(-1, 2)
+        r.body_xy = _dp(body)
+        r._body = body  # keeps the array alive while the request is
+    r.chord, r.far_radius, r.first_spacing = float(chord), float(far_radius), float(first_spacing)
+    r.grid_iters, r.init_mode = int(grid_iters), _lib.INIT[init]
+    r.params = p
+    r.residual_drop, r.max_steps = float(residual_drop), int(max_steps)
+    return r
+
+
+def request_bytes(r) -> float:
+    b = C.c_double()
+    check(lib().ausm_request_bytes(C.byref(r), C.byref(b)))
+    return b.value
+
+
+class Server:
+    """Continuous-batching solve server (no counterpart in the reference): requests are
+    admitted in arrival order by HBM budget and slots, stepped together in rounds of
+    `chunk_steps` RK3 steps, and retired at their own stopping rule."""
+
+    def __init__(self, hbm_budget_bytes: float = 160e9, max_active: int = 256, chunk_steps: int = 100,
+                 plain: bool = False, graphs: bool = True):
+        s = C.c_void_p()
+        flags = (_lib.SERVE_PLAIN if plain else 0) | (0 if graphs else _lib.SERVE_NO_GRAPH)
+        check(lib().ausm_server_create(float(hbm_budget_bytes), int(max_active), int(chunk_steps), flags,
+                                       C.byref(s)))
+        self.s = s
+        self._M = {}
+
+    def close(self):
+        if getattr(self, "s", None):
+            lib().ausm_server_destroy(self.s)
+            self.s = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _c(self, rc):
+        return check(rc, server=self.s)
+
+    def submit(self, r) -> int:
+        i = C.c_int64()
+        self._c(lib().ausm_server_submit(self.s, C.byref(r), C.byref(i)))
+        self._M[i.value] = r.M
+        return i.value
+
+    def pump(self) -> int:
+        left = C.c_int()
+        self._c(lib().ausm_server_pump(self.s, C.byref(left)))
+        return left.value
+
+    def start(self):
+        self._c(lib().ausm_server_start(self.s))
+
+    def stop(self):
+        self._c(lib().ausm_server_stop(self.s))
+
+    def drain(self, timeout_s: float | None = None):
+        self._c(lib().ausm_server_drain(self.s, -1.0 if timeout_s is None else timeout_s * 1e3))
+
+    def poll(self, rid: int, with_cp: bool = True) -> dict:
+        res = _lib.AusmResult()
+        cp = np.full(self._M.get(rid, 0), np.nan) if with_cp else None
+        self._c(lib().ausm_server_poll(self.s, int(rid), C.byref(res),
+                                       _dp(cp) if cp is not None and cp.size else None))
+        d = {k: getattr(res, k) for k, _ in res._fields_ if k != "forces"}
+        d.update(zip(("Fx", "Fy", "F", "Cl", "Cd", "ClCd"), list(res.forces)))
+        if with_cp:
+            d["Cp"] = cp
+        return d
+
+    def stats(self) -> dict:
+        st = _lib.AusmServerStats()
+        self._c(lib().ausm_server_stats(self.s, C.byref(st)))
+        return {k: getattr(st, k) for k, _ in st._fields_}

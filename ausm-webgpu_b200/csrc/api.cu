@@ -208,7 +208,7 @@ int ausm_destroy(ausm_solver* h) {
   cudaSetDevice(h->dev);
   if (h->st) cudaStreamSynchronize(h->st);
   void* dptrs[] = {h->V, h->V2, h->Q[0], h->Q[1], h->Q[2], h->S[0], h->S[1], h->S[2], h->fx, h->fy, h->res,
-                   h->flen, h->area, h->staging, h->cp, h->wave, h->dt, h->dacc, h->move, h->err_flag};
+                   h->flen, h->area, h->staging, h->cp, h->wave, h->dt, h->dacc, h->parts, h->move, h->err_flag};
   for (void* d : dptrs)
     if (d) cudaFree(d);
   if (h->h_dt) cudaFreeHost(h->h_dt);
@@ -258,6 +258,7 @@ int ausm_create(int M, int N, ausm_solver** out) {
   TRY(dalloc(&h->wave, 4));
   TRY(dalloc(&h->dt, 4));
   TRY(dalloc(&h->dacc, 4));
+  TRY(dalloc(&h->parts, 2 * (size_t)kMaxParts));
   TRY(dalloc(&h->move, 4));
   TRY(dalloc(&h->err_flag, 1));
   TRY(cudaMemsetAsync(h->err_flag, 0, sizeof(int), h->st));
@@ -660,8 +661,8 @@ int ausm_forces(ausm_solver* h, double* out6, double* cp) {
   double vx = h->speed_now * std::cos(a), vy = h->speed_now * std::sin(a);
   double q_inf = 0.5 * p.in_rho * (vx * vx + vy * vy);
   if (cp && !h->cp) CU(h, dalloc(&h->cp, (size_t)h->M));
-  CU(h, cudaMemsetAsync(h->dacc, 0, 2 * sizeof(double), h->st));
-  launch_forces(interior(h), h->V, h->c, h->M, h->dacc, cp ? h->cp : nullptr, q_inf, p.in_pressure, h->st);
+  launch_forces(interior(h), h->V, h->c, h->M, h->dacc, h->parts, cp ? h->cp : nullptr, q_inf, p.in_pressure,
+                h->st);
   CHECK_LAUNCH(h);
   CU(h, cudaMemcpyAsync(h->h_acc, h->dacc, 2 * sizeof(double), cudaMemcpyDeviceToHost, h->st));
   if (cp) CU(h, cudaMemcpyAsync(cp, h->cp, (size_t)h->M * sizeof(double), cudaMemcpyDeviceToHost, h->st));
@@ -702,8 +703,7 @@ int ausm_residual_l2(ausm_solver* h, double* l2) {
     launch_ref_residual(h->fx, h->fy, h->flen, h->area, h->res, M, N, h->st);
     R = h->res;
   }
-  CU(h, cudaMemsetAsync(h->dacc, 0, sizeof(double), h->st));
-  launch_sumsq_rho(R, (size_t)M * N, h->dacc, h->st);
+  launch_sumsq_rho(R, (size_t)M * N, h->dacc, h->parts, h->st);
   CHECK_LAUNCH(h);
   CU(h, cudaMemcpyAsync(h->h_acc, h->dacc, sizeof(double), cudaMemcpyDeviceToHost, h->st));
   CU(h, cudaStreamSynchronize(h->st));

@@ -29,8 +29,10 @@ __device__ __forceinline__ void block_max_to(uint32_t* dst, uint32_t v) {
   }
 }
 
-// Block-wide sum of doubles into dst (one atomicAdd per block).  All threads call it.
-__device__ __forceinline__ void block_sum_to(double* dst, double v) {
+// Block-wide sum of doubles, stored by one thread into *dst (a per-block slot; the
+// slots are then summed in a fixed order by launch_sum_parts, so the total does not
+// depend on block timing).  All threads call it.
+__device__ __forceinline__ void block_sum_store(double* dst, double v) {
   __shared__ double warp_sum[32];
   for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
   const int t = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
@@ -41,9 +43,11 @@ __device__ __forceinline__ void block_sum_to(double* dst, double v) {
     const int nw = (blockDim.x * blockDim.y * blockDim.z + 31) >> 5;
     double x = lane < nw ? warp_sum[lane] : 0.0;
     for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
-    if (lane == 0) atomicAdd(dst, x);
+    if (lane == 0) *dst = x;
   }
 }
+// Per-block partial sums of a reduction (at most kMaxParts blocks per quantity).
+constexpr int kMaxParts = 148 * 16;
 
 // ---- fused engine (kernels_fused.cu) ----
 // TMA descriptors of one solve: per state buffer the halo box (36 x 20 cells) and the
@@ -118,9 +122,10 @@ void launch_fill(float4* Q, float4 v, size_t n, cudaStream_t s);
 void launch_grid_init(float2* V, int M, int N, double first_spacing, cudaStream_t s);
 void launch_grid_jacobi(const float2* src, float2* dst, int M, int N, cudaStream_t s);
 void launch_grid_multicolor(float2* V, int M, int N, int color, float omega, uint32_t* move, cudaStream_t s);
-void launch_forces(const float4* row0, const float2* V, const Consts& c, int M, double* acc /*2*/, double* cp,
-                   double q_inf, double p_inf, cudaStream_t s);
-void launch_sumsq_rho(const float4* R, size_t n, double* acc, cudaStream_t s);
+// parts: 2 * kMaxParts doubles of scratch; acc gets the sums, in a fixed order.
+void launch_forces(const float4* row0, const float2* V, const Consts& c, int M, double* acc /*2*/, double* parts,
+                   double* cp, double q_inf, double p_inf, cudaStream_t s);
+void launch_sumsq_rho(const float4* R, size_t n, double* acc, double* parts, cudaStream_t s);
 void launch_field(const float4* Qint, const float2* V, const Consts& c, int kind, int M, int N, float* out,
                   cudaStream_t s);
 

@@ -103,7 +103,7 @@ __global__ void k_grid_multicolor(float2* __restrict__ V, int M, int N, int colo
 // ---- surface force (graphs.js:186-272): FP32 pressure of the first interior cell,
 // FP64 face length, normal and sum; also Cp per wall face ----
 __global__ void k_forces(const float4* __restrict__ row0, const float2* __restrict__ V, const Consts c, int M,
-                         double* acc, double* cp, double q_inf, double p_inf) {
+                         double* parts, double* cp, double q_inf, double p_inf) {
   double fx = 0.0, fy = 0.0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < M; i += gridDim.x * blockDim.x) {
     float4 s = row0[i];
@@ -117,18 +117,35 @@ __global__ void k_forces(const float4* __restrict__ row0, const float2* __restri
     fy += -(double)p * len * ny;
     if (cp) cp[i] = ((double)p - p_inf) / q_inf;
   }
-  block_sum_to(acc, fx);
+  block_sum_store(parts + blockIdx.x, fx);
   __syncthreads();
-  block_sum_to(acc + 1, fy);
+  block_sum_store(parts + kMaxParts + blockIdx.x, fy);
 }
 
-__global__ void k_sumsq_rho(const float4* __restrict__ R, size_t n, double* acc) {
+__global__ void k_sumsq_rho(const float4* __restrict__ R, size_t n, double* parts) {
   double s = 0.0;
   for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
     double r = R[k].x;
     s += r * r;
   }
-  block_sum_to(acc, s);
+  block_sum_store(parts + blockIdx.x, s);
+}
+
+// out[q] = sum of parts[q * kMaxParts + 0 .. nb - 1], in a fixed order (one block of
+// 256 threads per quantity q: strided partial sums, then a shared-memory tree).
+__global__ void k_sum_parts(const double* __restrict__ parts, int nb, double* __restrict__ out) {
+  __shared__ double sh[256];
+  const int t = threadIdx.x;
+  const double* p = parts + (size_t)blockIdx.x * kMaxParts;
+  double a = 0.0;
+  for (int k = t; k < nb; k += 256) a += p[k];
+  sh[t] = a;
+  __syncthreads();
+  for (int w = 128; w > 0; w >>= 1) {
+    if (t < w) sh[t] += sh[t + w];
+    __syncthreads();
+  }
+  if (t == 0) out[blockIdx.x] = sh[0];
 }
 
 // ---- headless field output (ausm.js:617-707 without the colour map) ----
@@ -186,13 +203,16 @@ void launch_grid_jacobi(const float2* src, float2* dst, int M, int N, cudaStream
 void launch_grid_multicolor(float2* V, int M, int N, int color, float omega, uint32_t* move, cudaStream_t s) {
   k_grid_multicolor<<<grid16(M, N + 1), B16, 0, s>>>(V, M, N, color, omega, move);
 }
-void launch_forces(const float4* row0, const float2* V, const Consts& c, int M, double* acc, double* cp,
-                   double q_inf, double p_inf, cudaStream_t s) {
+void launch_forces(const float4* row0, const float2* V, const Consts& c, int M, double* acc, double* parts,
+                   double* cp, double q_inf, double p_inf, cudaStream_t s) {
   int blocks = std::min((M + 255) / 256, 148);
-  k_forces<<<blocks, 256, 0, s>>>(row0, V, c, M, acc, cp, q_inf, p_inf);
+  k_forces<<<blocks, 256, 0, s>>>(row0, V, c, M, parts, cp, q_inf, p_inf);
+  k_sum_parts<<<2, 256, 0, s>>>(parts, blocks, acc);
 }
-void launch_sumsq_rho(const float4* R, size_t n, double* acc, cudaStream_t s) {
-  k_sumsq_rho<<<grid1d(n), 256, 0, s>>>(R, n, acc);
+void launch_sumsq_rho(const float4* R, size_t n, double* acc, double* parts, cudaStream_t s) {
+  const int blocks = grid1d(n);  // <= kMaxParts
+  k_sumsq_rho<<<blocks, 256, 0, s>>>(R, n, parts);
+  k_sum_parts<<<1, 256, 0, s>>>(parts, blocks, acc);
 }
 void launch_field(const float4* Qint, const float2* V, const Consts& c, int kind, int M, int N, float* out,
                   cudaStream_t s) {

@@ -31,6 +31,7 @@ struct ausm_solver {
   uint32_t* wave = nullptr;
   float* dt = nullptr;
   double* dacc = nullptr;
+  double* parts = nullptr;  // 2 * kMaxParts per-block partial sums
   uint32_t* move = nullptr;
   int* err_flag = nullptr;  // set by a kernel whose bounded wait gave up
   ausm::TmaMaps tma;

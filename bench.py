@@ -148,6 +148,83 @@ def build_solver(ausm, wl, engine="fused", M=None, N=None):
     return s
 
 
+# Served stream: Poisson arrivals at `rate` req/s; each request a random NACA 4-digit
+# airfoil (as in BATCH), grid cells log-uniform 16k-1M (aspect 4:3), Mach U[0.3, 6],
+# AoA U[-4, 8] deg, scheme uniform; stop at a 4-decade density-residual drop or 50000
+# steps; admission by a 160 GB HBM budget.  The stream is a bounded sample of
+# `requests` arrivals (the full 10000-request stream is hours of GPU time).
+SERVE = dict(name="served_poisson", seed=20261203, requests=32, rate=200.0, cells_lo=16384, cells_hi=1 << 20,
+             residual_drop=4.0, max_steps=50000, chunk=100, budget=160e9, slots=256, far_chords=20.0,
+             first_spacing=1e-3, grid_iters=200)
+
+
+def serve_stream(cfg):
+    import numpy as np
+    rng = np.random.default_rng(cfg["seed"] + 1)
+    n = cfg["requests"]
+    arrivals = np.cumsum(rng.exponential(1.0 / cfg["rate"], n))
+    lo, hi = math.log(cfg["cells_lo"]), math.log(cfg["cells_hi"])
+    out = []
+    for k in range(n):
+        cells = math.exp(rng.uniform(lo, hi))
+        M = max(16, int(round(math.sqrt(cells * 4.0 / 3.0) / 2)) * 2)
+        N = max(12, int(round(M * 0.75)))
+        m, pos, t = int(rng.integers(0, 7)), int(rng.integers(2, 7)), int(rng.integers(8, 19))
+        out.append(dict(t=float(arrivals[k]), M=M, N=N, naca=m * 1000 + (pos * 100 if m else 0) + t,
+                        mach=float(rng.uniform(0.3, 6.0)), aoa=float(rng.uniform(-4.0, 8.0)),
+                        scheme=int(rng.integers(0, 3))))
+    return out
+
+
+def run_served(ausm, cfg, plain):
+    """Submits the stream at its arrival times to a server (worker thread) and waits
+    for every result; latency = submit -> result ready."""
+    import numpy as np
+    stream = serve_stream(cfg)
+    srv = ausm.Server(cfg["budget"], cfg["slots"], cfg["chunk"], plain=plain)
+    srv.start()
+    ids = []
+    t0 = time.perf_counter()
+    for sp in stream:
+        delay = sp["t"] - (time.perf_counter() - t0)
+        if delay > 0:
+            time.sleep(delay)
+        r = ausm.make_request(sp["M"], sp["N"], naca4=sp["naca"], chord=1.0, far_radius=cfg["far_chords"],
+                              first_spacing=cfg["first_spacing"], grid_iters=cfg["grid_iters"],
+                              residual_drop=cfg["residual_drop"], max_steps=cfg["max_steps"], mach=sp["mach"],
+                              aoa_deg=sp["aoa"], scheme=sp["scheme"])
+        ids.append(srv.submit(r))
+    srv.drain()
+    wall = time.perf_counter() - t0
+    res = [srv.poll(i) for i in ids]
+    st = srv.stats()
+    srv.stop()
+    srv.close()
+    lat = np.array([r["latency_ms"] for r in res])
+    done = [r for r in res if r["state"] == 0]
+    return {"solves_per_s": len(done) / wall, "wall_s": wall, "p50_ms": float(np.percentile(lat, 50)),
+            "p99_ms": float(np.percentile(lat, 99)), "finished": len(done), "failed": len(res) - len(done),
+            "converged": sum(1 for r in done if r["stop"] == 1), "max_steps": sum(1 for r in done if r["stop"] == 2),
+            "steps_mean": float(np.mean([r["steps"] for r in res])), "rounds": st["rounds"],
+            "mcell_updates_per_s": st["cell_updates"] / wall / 1e6, "peak_gb": st["peak_bytes"] / 1e9}, res
+
+
+def run_serve_mode(ausm, cfg):
+    served, rs = run_served(ausm, cfg, plain=False)
+    plain, rp = run_served(ausm, cfg, plain=True)
+    err = 0.0
+    for a, b in zip(rs, rp):
+        if a["state"] == 0 and b["state"] == 0:
+            err = max(err, float(abs(a["Cp"] - b["Cp"]).max() / max(abs(b["Cp"]).max(), 1e-30)))
+    return {"metric": "served solves/s", "value": served["solves_per_s"], "unit": "solves/s",
+            "workload": cfg["name"], "requests": cfg["requests"], "rate_per_s": cfg["rate"],
+            "p50_ms": served["p50_ms"], "p99_ms": served["p99_ms"], "served": served,
+            "plain_one_solve_at_a_time": plain, "speedup_vs_plain": served["solves_per_s"] / plain["solves_per_s"],
+            "cp_max_rel_diff_vs_plain": err,
+            "config": {k: cfg[k] for k in ("seed", "requests", "rate", "residual_drop", "max_steps", "chunk",
+                                           "budget", "slots")}}
+
+
 def batch_specs(cfg):
     import numpy as np
     rng = np.random.default_rng(cfg["seed"])
@@ -327,9 +404,12 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--small", action="store_true", help="512x384 grid (profiling and quick checks)")
-    ap.add_argument("--mode", default="step", choices=["step", "batch"],
+    ap.add_argument("--mode", default="step", choices=["step", "batch", "serve"],
                     help="step: the 4096x3072 step (headline line, with the batched measurement "
-                         "attached); batch: the batched measurement alone")
+                         "attached); batch: the batched measurement alone; serve: the served stream")
+    ap.add_argument("--serve-requests", type=int, default=SERVE["requests"])
+    ap.add_argument("--serve-rate", type=float, default=SERVE["rate"])
+    ap.add_argument("--serve-max-steps", type=int, default=SERVE["max_steps"])
     ap.add_argument("--no-batch", action="store_true", help="skip the batched measurement in --mode step")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -348,6 +428,12 @@ def main():
     ausm.set_device(local_rank)
     if args.mode == "batch":
         res = run_batched(ausm, BATCH, args.warmup)
+        if rank == 0:
+            print(json.dumps(res))
+        return 0
+    if args.mode == "serve":
+        cfg = dict(SERVE, requests=args.serve_requests, rate=args.serve_rate, max_steps=args.serve_max_steps)
+        res = run_serve_mode(ausm, cfg)
         if rank == 0:
             print(json.dumps(res))
         return 0

@@ -220,6 +220,89 @@ int ausm_batch_synchronize(ausm_batch* b);
  * elapsed device time of all of them. */
 int ausm_batch_time_steps(ausm_batch* b, int n, int reps, float* ms_out);
 
+/* ---- serving: continuous batching of solve requests (no counterpart in the reference) ----
+ * A server admits requests (airfoil, grid size, flow, scheme, stopping rule) as they
+ * arrive, in arrival order, while the HBM budget and the slot count allow; keeps their
+ * state resident on the device in one batch; advances the batch in rounds of
+ * `chunk_steps` RK3 steps (dt held per round, as one reference frame); after each round
+ * checks every member's density-residual L2 norm (FP64) against its own stopping rule
+ * and retires the finished ones with their forces and surface Cp (FP64), freeing their
+ * memory for the next arrivals.  A request's steps are counted from its admission, so
+ * its result is the same whether it runs alone or among others.  Requests are rejected
+ * at submit on the host (invalid or non-finite fields: AUSM_ERR_INVALID; larger than
+ * the whole budget: AUSM_ERR_BUDGET).  A request that diverges ends with state
+ * AUSM_ERR_DIVERGED and does not affect the others. */
+typedef struct AusmRequest {
+  int M, N;              /* cells around the body (periodic) x radial */
+  int naca4;             /* NACA 4-digit code, used when body_xy is NULL */
+  int closed_te;         /* 1: closed trailing edge (-0.1036 coefficient) */
+  const double* body_xy; /* optional M body vertices (x, y) from a .dat loader; copied */
+  double chord;          /* NACA chord; the body spans x in [-chord/2, chord/2] */
+  double far_radius;     /* circular far field radius, centred at the origin */
+  double first_spacing;  /* first radial cell height of the initial grid; 0 = uniform */
+  int grid_iters;        /* multicolor TTM sweeps */
+  int init_mode;         /* AUSM_INIT_* */
+  AusmParams params;
+  double residual_drop;  /* stop after this many decades of density-residual L2 drop */
+  int max_steps;         /* ... or after this many RK3 steps (rounded up to whole rounds) */
+} AusmRequest;
+
+#define AUSM_REQ_DONE 0    /* state: finished (see stop) */
+#define AUSM_REQ_QUEUED 1  /* state: waiting for admission */
+#define AUSM_REQ_RUNNING 2 /* state: on the device */
+#define AUSM_STOP_CONVERGED 1
+#define AUSM_STOP_MAX_STEPS 2
+#define AUSM_STOP_DIVERGED 3
+
+typedef struct AusmResult {
+  int64_t id;
+  int state;      /* AUSM_REQ_* or a negative status (the request failed) */
+  int stop;       /* AUSM_STOP_* once finished */
+  int M, N;
+  int steps;      /* RK3 steps taken */
+  double l2_first; /* density-residual L2 of the initial state */
+  double l2_last;  /* ... after the last round */
+  double forces[6]; /* Fx, Fy, |F| sign, Cl, Cd, Cl/Cd as ausm_forces */
+  double queue_ms;  /* submit -> admission */
+  double run_ms;    /* admission -> finished */
+  double latency_ms; /* submit -> finished */
+} AusmResult;
+
+typedef struct AusmServerStats {
+  int64_t submitted, rejected, admitted, finished, failed, rounds;
+  int pending, active;
+  double bytes_in_use, peak_bytes, cell_updates;
+} AusmServerStats;
+
+#define AUSM_SERVE_PLAIN 1   /* flag: no batch; one solve at a time, ausm_step per round */
+#define AUSM_SERVE_NO_GRAPH 2 /* flag: batch without CUDA graphs */
+
+typedef struct ausm_server ausm_server;
+/* New server on the current device.  hbm_budget_bytes: device memory its solves may
+ * hold at once; max_active: slots (concurrent solves); chunk_steps: RK3 steps per round.
+ * No CUDA call happens until the first round. */
+int ausm_server_create(double hbm_budget_bytes, int max_active, int chunk_steps, int flags, ausm_server** out);
+int ausm_server_destroy(ausm_server* s);
+const char* ausm_server_last_error(const ausm_server* s);
+/* Device bytes a request holds while admitted (what admission charges to the budget). */
+int ausm_request_bytes(const AusmRequest* r, double* bytes);
+/* Queues a request; *id identifies it.  Thread-safe. */
+int ausm_server_submit(ausm_server* s, const AusmRequest* r, int64_t* id);
+/* One round on the calling thread: admit, step, check, retire.  *active gets the
+ * number of solves left on the device or queued.  Use either this or the worker. */
+int ausm_server_pump(ausm_server* s, int* remaining);
+/* Starts / stops a worker thread that pumps whenever requests are queued or active. */
+int ausm_server_start(ausm_server* s);
+int ausm_server_stop(ausm_server* s);
+/* Result of request id (state AUSM_REQ_QUEUED / RUNNING until done); cp (may be NULL)
+ * gets the M wall Cp values once done.  AUSM_ERR_NOT_FOUND for an unknown id. */
+int ausm_server_poll(ausm_server* s, int64_t id, AusmResult* res, double* cp);
+/* Waits until nothing is queued or active (the worker must be running, or the call
+ * pumps on this thread); timeout_ms < 0 waits without limit.  AUSM_ERR_TIMEOUT if the
+ * time ran out first. */
+int ausm_server_drain(ausm_server* s, double timeout_ms);
+int ausm_server_stats(ausm_server* s, AusmServerStats* st);
+
 #ifdef __cplusplus
 }
 #endif
