@@ -111,7 +111,7 @@ const float4* interior(ausm_solver* h) {
 int refresh_wave(ausm_solver* h) {
   CU(h, cudaMemsetAsync(h->wave, 0, sizeof(uint32_t), h->st));
   if (h->engine == AUSM_ENGINE_FUSED) {
-    launch_wave_interior(h->Q[h->cur], h->V, h->c.gamma, h->M, h->N, h->wave, h->st);
+    launch_wave_interior(h->Q[h->cur], h->Mj, h->c.gamma, h->M, h->N, h->wave, h->st);
   } else {
     launch_ref_wave(h->S[2], h->flen, h->area, h->c.gamma, h->M, h->N, h->wave, h->st);
   }
@@ -120,6 +120,8 @@ int refresh_wave(ausm_solver* h) {
 }
 
 int after_grid(ausm_solver* h) {
+  launch_metrics_d(h->Vd, h->Mi, h->Mj, h->M, h->N, h->st);
+  CHECK_LAUNCH(h);
   if (h->engine == AUSM_ENGINE_REFERENCE) {
     launch_ref_metrics(h->V, h->area, h->flen, h->M, h->N, h->st);
     CHECK_LAUNCH(h);
@@ -207,7 +209,7 @@ int ausm_destroy(ausm_solver* h) {
   if (h->batch) ausm_batch_remove(h->batch, h);
   cudaSetDevice(h->dev);
   if (h->st) cudaStreamSynchronize(h->st);
-  void* dptrs[] = {h->V, h->V2, h->Q[0], h->Q[1], h->Q[2], h->S[0], h->S[1], h->S[2], h->fx, h->fy, h->res,
+  void* dptrs[] = {h->V, h->V2, h->Vd, h->Mi, h->Mj, h->Q[0], h->Q[1], h->Q[2], h->S[0], h->S[1], h->S[2], h->fx, h->fy, h->res,
                    h->flen, h->area, h->staging, h->cp, h->wave, h->dt, h->dacc, h->parts, h->move, h->err_flag};
   for (void* d : dptrs)
     if (d) cudaFree(d);
@@ -254,6 +256,9 @@ int ausm_create(int M, int N, ausm_solver** out) {
   TRY(cudaEventCreate(&h->e1));
   size_t n = (size_t)M * N;
   TRY(dalloc(&h->V, (size_t)M * (N + 1)));
+  TRY(dalloc(&h->Vd, (size_t)M * (N + 1)));
+  TRY(dalloc(&h->Mi, n));
+  TRY(dalloc(&h->Mj, (size_t)M * (N + 1)));
   for (auto& q : h->Q) TRY(dalloc(&q, n));
   TRY(dalloc(&h->wave, 4));
   TRY(dalloc(&h->dt, 4));
@@ -271,7 +276,7 @@ int ausm_create(int M, int N, ausm_solver** out) {
     const float4* qs[3] = {h->Q[0], h->Q[1], h->Q[2]};
     // odd M keeps the per-thread staging kernel; AUSM_NO_TMA=1 selects it for A/B timing
     const char* no_tma = std::getenv("AUSM_NO_TMA");
-    if (!(no_tma && no_tma[0] == '1')) encode_tma_maps(qs, h->V, M, N, &h->tma);
+    if (!(no_tma && no_tma[0] == '1')) encode_tma_maps(qs, h->Mi, h->Mj, M, N, &h->tma);
   }
   ausm_default_params(&h->p);
   h->speed_now = inflow_target(h->p);
@@ -440,19 +445,19 @@ int ausm_generate_grid(ausm_solver* h, int iters, int method, double tol, int* i
   int rc = use_device(h);
   if (rc) return rc;
   const int M = h->M, N = h->N;
-  std::vector<float> v((size_t)M * (N + 1) * 2, 0.0f);
-  for (int i = 0; i < M; i++) {
-    v[2 * i] = (float)h->body[2 * i];
-    v[2 * i + 1] = (float)h->body[2 * i + 1];
-    size_t o = ((size_t)N * M + i) * 2;
-    v[o] = (float)h->outer[2 * i];
-    v[o + 1] = (float)h->outer[2 * i + 1];
-  }
-  CU(h, cudaMemcpyAsync(h->V, v.data(), v.size() * sizeof(float), cudaMemcpyHostToDevice, h->st));
-  launch_grid_init(h->V, M, N, h->stretch, h->st);
-  CHECK_LAUNCH(h);
   int done = 0;
-  if (method == AUSM_GRID_JACOBI) {
+  if (method == AUSM_GRID_JACOBI) {  // FP32, the reference's generator (shaders/grid.js:33-113)
+    std::vector<float> v((size_t)M * (N + 1) * 2, 0.0f);
+    for (int i = 0; i < M; i++) {
+      v[2 * i] = (float)h->body[2 * i];
+      v[2 * i + 1] = (float)h->body[2 * i + 1];
+      size_t o = ((size_t)N * M + i) * 2;
+      v[o] = (float)h->outer[2 * i];
+      v[o + 1] = (float)h->outer[2 * i + 1];
+    }
+    CU(h, cudaMemcpyAsync(h->V, v.data(), v.size() * sizeof(float), cudaMemcpyHostToDevice, h->st));
+    launch_grid_init(h->V, M, N, h->stretch, h->st);
+    CHECK_LAUNCH(h);
     if (iters > 0) {
       if (!h->V2) CU(h, dalloc(&h->V2, (size_t)M * (N + 1)));
       CU(h, cudaMemcpyAsync(h->V2, h->V, (size_t)M * (N + 1) * sizeof(float2), cudaMemcpyDeviceToDevice, h->st));
@@ -465,13 +470,25 @@ int ausm_generate_grid(ausm_solver* h, int iters, int method, double tol, int* i
       if (src != h->V)
         CU(h, cudaMemcpyAsync(h->V, src, (size_t)M * (N + 1) * sizeof(float2), cudaMemcpyDeviceToDevice, h->st));
     }
+    launch_f2d(h->V, h->Vd, (size_t)M * (N + 1), h->st);
     done = iters;
-  } else {
+  } else {  // FP64 multicolor Gauss-Seidel from the FP64 boundaries
+    std::vector<double> vd((size_t)M * (N + 1) * 2, 0.0);
+    for (int i = 0; i < M; i++) {
+      vd[2 * i] = h->body[2 * i];
+      vd[2 * i + 1] = h->body[2 * i + 1];
+      size_t o = ((size_t)N * M + i) * 2;
+      vd[o] = h->outer[2 * i];
+      vd[o + 1] = h->outer[2 * i + 1];
+    }
+    CU(h, cudaMemcpyAsync(h->Vd, vd.data(), vd.size() * sizeof(double), cudaMemcpyHostToDevice, h->st));
+    launch_grid_init_d(h->Vd, M, N, h->stretch, h->st);
+    CHECK_LAUNCH(h);
     const int ncol = (M & 1) ? 6 : 4;
     const int check_every = 25;
     for (int it = 0; it < iters; it++) {
       CU(h, cudaMemsetAsync(h->move, 0, sizeof(uint32_t), h->st));
-      for (int col = 0; col < ncol; col++) launch_grid_multicolor(h->V, M, N, col, 1.0f, h->move, h->st);
+      for (int col = 0; col < ncol; col++) launch_grid_multicolor_d(h->Vd, M, N, col, 1.0, h->move, h->st);
       done = it + 1;
       if (tol > 0.0 && (done % check_every == 0 || done == iters)) {
         CHECK_LAUNCH(h);
@@ -483,7 +500,9 @@ int ausm_generate_grid(ausm_solver* h, int iters, int method, double tol, int* i
       }
     }
     CHECK_LAUNCH(h);
+    launch_d2f(h->Vd, h->V, (size_t)M * (N + 1), h->st);
   }
+  CHECK_LAUNCH(h);
   if (iters_done) *iters_done = done;
   return after_grid(h);
 }
@@ -494,6 +513,7 @@ int ausm_set_vertices(ausm_solver* h, const float* xy) {
   int rc = use_device(h);
   if (rc) return rc;
   CU(h, cudaMemcpyAsync(h->V, xy, (size_t)h->M * (h->N + 1) * sizeof(float2), cudaMemcpyHostToDevice, h->st));
+  launch_f2d(h->V, h->Vd, (size_t)h->M * (h->N + 1), h->st);
   return after_grid(h);
 }
 
@@ -587,16 +607,16 @@ int ausm_step(ausm_solver* h, int n, float* dt_out) {
         TmaMapsLaunch t1, t2, t3;
         const TmaMapsLaunch *p1 = nullptr, *p2 = nullptr, *p3 = nullptr;
         if (h->tma.ok) {
-          t1 = {h->tma.halo[a], h->tma.plain[a], h->tma.v};
-          t2 = {h->tma.halo[b], h->tma.plain[a], h->tma.v};
-          t3 = {h->tma.halo[c3], h->tma.plain[a], h->tma.v};
+          t1 = {h->tma.halo[a], h->tma.plain[a], h->tma.mi, h->tma.mj};
+          t2 = {h->tma.halo[b], h->tma.plain[a], h->tma.mi, h->tma.mj};
+          t3 = {h->tma.halo[c3], h->tma.plain[a], h->tma.mi, h->tma.mj};
           p1 = &t1; p2 = &t2; p3 = &t3;
         }
-        launch_fused_stage(sch, 1, false, h->Q[a], nullptr, h->Q[b], h->V, h->dt, h->wave, h->c, M, N, p1,
+        launch_fused_stage(sch, 1, false, h->Q[a], nullptr, h->Q[b], h->Mi, h->Mj, h->dt, h->wave, h->c, M, N, p1,
                            h->err_flag, s);
-        launch_fused_stage(sch, 2, false, h->Q[b], h->Q[a], h->Q[c3], h->V, h->dt, h->wave, h->c, M, N, p2,
+        launch_fused_stage(sch, 2, false, h->Q[b], h->Q[a], h->Q[c3], h->Mi, h->Mj, h->dt, h->wave, h->c, M, N, p2,
                            h->err_flag, s);
-        launch_fused_stage(sch, 3, k == n - 1, h->Q[c3], h->Q[a], h->Q[b], h->V, h->dt, h->wave, h->c, M, N, p3,
+        launch_fused_stage(sch, 3, k == n - 1, h->Q[c3], h->Q[a], h->Q[b], h->Mi, h->Mj, h->dt, h->wave, h->c, M, N, p3,
                            h->err_flag, s);
         h->cur = b;
       }
@@ -661,7 +681,7 @@ int ausm_forces(ausm_solver* h, double* out6, double* cp) {
   double vx = h->speed_now * std::cos(a), vy = h->speed_now * std::sin(a);
   double q_inf = 0.5 * p.in_rho * (vx * vx + vy * vy);
   if (cp && !h->cp) CU(h, dalloc(&h->cp, (size_t)h->M));
-  launch_forces(interior(h), h->V, h->c, h->M, h->dacc, h->parts, cp ? h->cp : nullptr, q_inf, p.in_pressure,
+  launch_forces(interior(h), h->Vd, h->c, h->M, h->dacc, h->parts, cp ? h->cp : nullptr, q_inf, p.in_pressure,
                 h->st);
   CHECK_LAUNCH(h);
   CU(h, cudaMemcpyAsync(h->h_acc, h->dacc, 2 * sizeof(double), cudaMemcpyDeviceToHost, h->st));
@@ -694,7 +714,7 @@ int ausm_residual_l2(ausm_solver* h, double* l2) {
   const float4* R;
   if (h->engine == AUSM_ENGINE_FUSED) {
     float4* scratch = h->Q[(h->cur + 1) % 3];
-    launch_fused_stage(h->p.scheme, 0, false, h->Q[h->cur], nullptr, scratch, h->V, h->dt, h->wave, h->c, M, N,
+    launch_fused_stage(h->p.scheme, 0, false, h->Q[h->cur], nullptr, scratch, h->Mi, h->Mj, h->dt, h->wave, h->c, M, N,
                        nullptr, h->err_flag, h->st);
     R = scratch;
   } else {

@@ -51,26 +51,28 @@ constexpr int kMaxParts = 148 * 16;
 
 // ---- fused engine (kernels_fused.cu) ----
 // TMA descriptors of one solve: per state buffer the halo box (36 x 20 cells) and the
-// plain box (32 x 16 cells), and the vertex box (34 x 17).
+// plain box (32 x 16 cells), and the face-record boxes (33 x 16 i-faces, 32 x 17
+// j-faces).
 struct TmaMaps {
   CUtensorMap halo[3];
   CUtensorMap plain[3];
-  CUtensorMap v;
+  CUtensorMap mi, mj;
   bool ok = false;
 };
-struct TmaMapsLaunch {  // the three a stage launch reads
+struct TmaMapsLaunch {  // the four a stage launch reads
   CUtensorMap qs;
   CUtensorMap qn;
-  CUtensorMap v;
+  CUtensorMap mi, mj;
 };
-bool encode_tma_maps(const float4* const Q[3], const float2* V, int M, int N, TmaMaps* out);
+bool encode_tma_maps(const float4* const Q[3], const float4* Mi, const float4* Mj, int M, int N, TmaMaps* out);
 // stage 1..3: RK stage; stage 0: write dQ/dt of Qs to Qo.  emit (stage 3 only):
 // atomicMax the new state's wave speed bits into *wave (zeroed by the caller).  With
 // tm != nullptr the persistent TMA kernel runs and sets *err on a bounded-wait timeout.
+// Mi, Mj: the FP64-computed face records (launch_metrics_d).
 void launch_fused_stage(int scheme, int stage, bool emit, const float4* Qs, const float4* Qn, float4* Qo,
-                        const float2* V, const float* dt, uint32_t* wave, const Consts& c, int M, int N,
-                        const TmaMapsLaunch* tm, int* err, cudaStream_t s);
-void launch_wave_interior(const float4* Q, const float2* V, float gamma, int M, int N, uint32_t* wave,
+                        const float4* Mi, const float4* Mj, const float* dt, uint32_t* wave, const Consts& c, int M,
+                        int N, const TmaMapsLaunch* tm, int* err, cudaStream_t s);
+void launch_wave_interior(const float4* Q, const float4* Mj, float gamma, int M, int N, uint32_t* wave,
                           cudaStream_t s);
 
 // ---- batched engine (kernels_batch.cu) ----
@@ -79,7 +81,9 @@ void launch_wave_interior(const float4* Q, const float2* V, float gamma, int M, 
 // holding the current state (the RK3 buffers rotate by one per step).
 struct BatchSolve {
   float4* Q[3];
-  const float2* V;
+  const float4* Mi;
+  const float4* Mj;
+  const CUtensorMap* maps;  // in device memory: halo[0..2], plain[0..2], mi, mj; null without TMA
   float* dt;
   uint32_t* wave;
   Consts c;
@@ -89,8 +93,10 @@ struct BatchSolve {
 // Stage 0 writes the residual dQ/dt of the current state into the solve's next buffer.
 // A stage launch covers one scheme group: descriptors [s_lo, s_hi), items [t_lo, t_hi).
 void launch_batch_dt(BatchSolve* d, int nsolves, cudaStream_t s);
+// With err != nullptr (every solve of the launch has maps) stages 1-3 stage their tiles
+// by TMA and a bounded-wait timeout sets *err.
 void launch_batch_stage(int scheme, int stage, bool emit, const BatchSolve* d, int s_lo, int s_hi, int t_lo,
-                        int t_hi, int rot, cudaStream_t s);
+                        int t_hi, int rot, int* err, cudaStream_t s);
 void launch_batch_advance(BatchSolve* d, int nsolves, int steps, cudaStream_t s);
 // out[2 s] = dt, out[2 s + 1] = max wave speed of solve s
 void launch_batch_gather(const BatchSolve* d, int nsolves, float* out, cudaStream_t s);
@@ -123,7 +129,13 @@ void launch_grid_init(float2* V, int M, int N, double first_spacing, cudaStream_
 void launch_grid_jacobi(const float2* src, float2* dst, int M, int N, cudaStream_t s);
 void launch_grid_multicolor(float2* V, int M, int N, int color, float omega, uint32_t* move, cudaStream_t s);
 // parts: 2 * kMaxParts doubles of scratch; acc gets the sums, in a fixed order.
-void launch_forces(const float4* row0, const float2* V, const Consts& c, int M, double* acc /*2*/, double* parts,
+// FP64 grid and face records (kernels_misc.cu): see k_metrics_d for the record layout.
+void launch_grid_init_d(double2* V, int M, int N, double first_spacing, cudaStream_t s);
+void launch_grid_multicolor_d(double2* V, int M, int N, int color, double omega, uint32_t* move, cudaStream_t s);
+void launch_d2f(const double2* a, float2* b, size_t n, cudaStream_t s);
+void launch_f2d(const float2* a, double2* b, size_t n, cudaStream_t s);
+void launch_metrics_d(const double2* V, float4* Mi, float4* Mj, int M, int N, cudaStream_t s);
+void launch_forces(const float4* row0, const double2* V, const Consts& c, int M, double* acc /*2*/, double* parts,
                    double* cp, double q_inf, double p_inf, cudaStream_t s);
 void launch_sumsq_rho(const float4* R, size_t n, double* acc, double* parts, cudaStream_t s);
 void launch_field(const float4* Qint, const float2* V, const Consts& c, int kind, int M, int N, float* out,

@@ -45,7 +45,10 @@ struct ausm_batch {
   bool uploaded = false;
   int total_tiles = 0;
   BatchSolve* d_solves = nullptr;
-  int cap = 0;  // descriptor capacity of d_solves / d_out / d_l2
+  CUtensorMap* d_maps = nullptr;  // 8 per descriptor (halo[3], plain[3], mi, mj) when tma
+  bool tma = false;               // every member has tensor maps: stages load tiles by TMA
+  int* d_err = nullptr;           // set by a TMA tile whose bounded wait gave up
+  int cap = 0;  // descriptor capacity of d_solves / d_maps / d_out / d_l2
   float* d_out = nullptr;
   double* d_l2 = nullptr;
   double* d_part = nullptr;
@@ -90,10 +93,12 @@ void drop_graphs(ausm_batch* b) {
   b->graph.clear();
 }
 
-BatchSolve describe(const ausm_solver* h, int tile0) {
+BatchSolve describe(const ausm_solver* h, int tile0, const CUtensorMap* maps) {
   BatchSolve d{};
+  d.maps = maps;
   for (int k = 0; k < 3; k++) d.Q[k] = h->Q[k];
-  d.V = h->V;
+  d.Mi = h->Mi;
+  d.Mj = h->Mj;
   d.dt = h->dt;
   d.wave = h->wave;
   d.c = h->c;
@@ -106,6 +111,8 @@ BatchSolve describe(const ausm_solver* h, int tile0) {
   return d;
 }
 
+const CUtensorMap* maps_of(const ausm_batch* b, int k) { return b->tma ? b->d_maps + 8 * (size_t)k : nullptr; }
+
 // Grows the per-member and per-tile device arrays (dropping graphs that point at them).
 int ensure_capacity(ausm_batch* b) {
   const int n = (int)b->members.size();
@@ -114,16 +121,18 @@ int ensure_capacity(ausm_batch* b) {
     if (b->cap) drop_graphs(b);
     BCU(b, cudaStreamSynchronize(b->st));
     cudaFree(b->d_solves);
+    cudaFree(b->d_maps);
     cudaFree(b->d_out);
     cudaFree(b->d_l2);
     cudaFreeHost(b->h_out);
     cudaFreeHost(b->h_l2);
-    b->d_solves = nullptr; b->d_out = nullptr; b->d_l2 = nullptr; b->h_out = nullptr; b->h_l2 = nullptr;
+    b->d_solves = nullptr; b->d_maps = nullptr; b->d_out = nullptr; b->d_l2 = nullptr; b->h_out = nullptr; b->h_l2 = nullptr;
     b->cap = 0;
     BCU(b, cudaMalloc((void**)&b->d_solves, cap * sizeof(BatchSolve)));
+    BCU(b, cudaMalloc((void**)&b->d_maps, cap * 8 * sizeof(CUtensorMap)));
     BCU(b, cudaMalloc((void**)&b->d_out, cap * 2 * sizeof(float)));
     BCU(b, cudaMalloc((void**)&b->d_l2, cap * sizeof(double)));
-    BCU(b, cudaMallocHost((void**)&b->h_out, cap * 2 * sizeof(float)));
+    BCU(b, cudaMallocHost((void**)&b->h_out, (cap * 2 + 1) * sizeof(float)));  // + the error flag
     BCU(b, cudaMallocHost((void**)&b->h_l2, cap * sizeof(double)));
     b->cap = cap;
     b->uploaded = false;
@@ -154,11 +163,13 @@ void relayout(ausm_batch* b) {
   });
   int t = 0;
   b->groups.clear();
+  b->tma = !b->members.empty();
+  for (ausm_solver* h : b->members) b->tma = b->tma && h->tma.ok;
   for (int k : b->order) {
     const ausm_solver* h = b->members[k];
     const int s = (int)b->mirror.size();
     if (b->groups.empty() || b->groups.back().scheme != h->p.scheme) b->groups.push_back({h->p.scheme, s, s, t, t});
-    b->mirror.push_back(describe(h, t));
+    b->mirror.push_back(describe(h, t, maps_of(b, s)));
     t += ((h->M + kTX - 1) / kTX) * ((h->N + kTY - 1) / kTY);
     b->groups.back().s_hi = s + 1;
     b->groups.back().t_hi = t;
@@ -176,7 +187,7 @@ int sync_descriptors(ausm_batch* b) {
     }
   bool changed = !b->uploaded;
   for (size_t k = 0; k < b->members.size(); k++) {
-    BatchSolve d = describe(b->members[b->order[k]], b->mirror[k].tile0);
+    BatchSolve d = describe(b->members[b->order[k]], b->mirror[k].tile0, maps_of(b, (int)k));
     if (std::memcmp(&d, &b->mirror[k], sizeof d) != 0) {
       b->mirror[k] = d;
       changed = true;
@@ -186,6 +197,19 @@ int sync_descriptors(ausm_batch* b) {
     // pageable source: the call returns once the source has been staged
     BCU(b, cudaMemcpyAsync(b->d_solves, b->mirror.data(), b->mirror.size() * sizeof(BatchSolve),
                            cudaMemcpyHostToDevice, b->st));
+    if (b->tma) {  // each member's maps, in work-list order
+      std::vector<CUtensorMap> maps;
+      maps.reserve(8 * b->members.size());
+      for (int k : b->order) {
+        const ausm::TmaMaps& t = b->members[k]->tma;
+        for (int q = 0; q < 3; q++) maps.push_back(t.halo[q]);
+        for (int q = 0; q < 3; q++) maps.push_back(t.plain[q]);
+        maps.push_back(t.mi);
+        maps.push_back(t.mj);
+      }
+      BCU(b, cudaMemcpyAsync(b->d_maps, maps.data(), maps.size() * sizeof(CUtensorMap), cudaMemcpyHostToDevice,
+                             b->st));
+    }
     b->uploaded = true;
   }
   return AUSM_OK;
@@ -195,6 +219,7 @@ int sync_descriptors(ausm_batch* b) {
 // the dt / wave gather
 void enqueue_steps(ausm_batch* b, int n) {
   const int ns = (int)b->members.size();
+  int* err = b->tma ? b->d_err : nullptr;
   ausm::launch_batch_dt(b->d_solves, ns, b->st);
   const int G = (int)b->groups.size();
   for (int g = 1; g < G; g++) {
@@ -205,9 +230,9 @@ void enqueue_steps(ausm_batch* b, int n) {
     const ausm_batch::Group& q = b->groups[g];
     cudaStream_t s = g == 0 ? b->st : b->aux[g - 1];
     for (int k = 0; k < n; k++) {
-      ausm::launch_batch_stage(q.scheme, 1, false, b->d_solves, q.s_lo, q.s_hi, q.t_lo, q.t_hi, k, s);
-      ausm::launch_batch_stage(q.scheme, 2, false, b->d_solves, q.s_lo, q.s_hi, q.t_lo, q.t_hi, k, s);
-      ausm::launch_batch_stage(q.scheme, 3, k == n - 1, b->d_solves, q.s_lo, q.s_hi, q.t_lo, q.t_hi, k, s);
+      ausm::launch_batch_stage(q.scheme, 1, false, b->d_solves, q.s_lo, q.s_hi, q.t_lo, q.t_hi, k, err, s);
+      ausm::launch_batch_stage(q.scheme, 2, false, b->d_solves, q.s_lo, q.s_hi, q.t_lo, q.t_hi, k, err, s);
+      ausm::launch_batch_stage(q.scheme, 3, k == n - 1, b->d_solves, q.s_lo, q.s_hi, q.t_lo, q.t_hi, k, err, s);
     }
   }
   for (int g = 1; g < G; g++) {
@@ -273,6 +298,8 @@ int ausm_batch_create(ausm_batch** out) {
   }
   e = cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming);
   if (e != cudaSuccess) return bail(e, "cudaEventCreate");
+  if ((e = cudaMalloc((void**)&b->d_err, 2 * sizeof(int))) != cudaSuccess) return bail(e, "cudaMalloc");
+  if ((e = cudaMemsetAsync(b->d_err, 0, 2 * sizeof(int), b->st)) != cudaSuccess) return bail(e, "cudaMemsetAsync");
   *out = b;
   return AUSM_OK;
 }
@@ -284,6 +311,8 @@ int ausm_batch_destroy(ausm_batch* b) {
   if (b->st) cudaStreamSynchronize(b->st);
   drop_graphs(b);
   cudaFree(b->d_solves);
+  cudaFree(b->d_maps);
+  cudaFree(b->d_err);
   cudaFree(b->d_out);
   cudaFree(b->d_l2);
   cudaFree(b->d_part);
@@ -370,7 +399,14 @@ int ausm_batch_step(ausm_batch* b, int n, float* dt_wave) {
   }
   if (!dt_wave) return AUSM_OK;
   BCU(b, cudaMemcpyAsync(b->h_out, b->d_out, ns * 2 * sizeof(float), cudaMemcpyDeviceToHost, b->st));
+  BCU(b, cudaMemcpyAsync(b->h_out + 2 * b->cap, b->d_err, sizeof(int), cudaMemcpyDeviceToHost, b->st));
   BCU(b, cudaStreamSynchronize(b->st));
+  int err_flag;
+  std::memcpy(&err_flag, b->h_out + 2 * b->cap, sizeof(int));
+  if (err_flag) {
+    BCU(b, cudaMemsetAsync(b->d_err, 0, sizeof(int), b->st));
+    return bfail(b, AUSM_ERR_TIMEOUT, "a tile load did not arrive within the bounded wait");
+  }
   for (int k = 0; k < ns; k++) {
     dt_wave[2 * b->order[k]] = b->h_out[2 * k];
     dt_wave[2 * b->order[k] + 1] = b->h_out[2 * k + 1];
@@ -390,7 +426,7 @@ int ausm_batch_residual_l2(ausm_batch* b, double* l2) {
   rc = sync_descriptors(b);
   if (rc) return rc;
   for (const ausm_batch::Group& q : b->groups)
-    ausm::launch_batch_stage(q.scheme, 0, false, b->d_solves, q.s_lo, q.s_hi, q.t_lo, q.t_hi, 0, b->st);
+    ausm::launch_batch_stage(q.scheme, 0, false, b->d_solves, q.s_lo, q.s_hi, q.t_lo, q.t_hi, 0, nullptr, b->st);
   ausm::launch_batch_residual_norm(b->d_solves, ns, b->total_tiles, b->d_part, b->d_l2, b->st);
   BCU(b, cudaGetLastError());
   BCU(b, cudaMemcpyAsync(b->h_l2, b->d_l2, ns * sizeof(double), cudaMemcpyDeviceToHost, b->st));

@@ -3,7 +3,8 @@
 // work list is the concatenation of all solves' 32 x 16 tiles, grouped by scheme; each
 // CTA takes one work item, finds its solve by binary search over the solves'
 // first-tile offsets, and runs the same tile compute as the single-solve kernel
-// (stage_tile.cuh) with that solve's buffers, constants and dt.  The scheme is a
+// (stage_tile.cuh) with that solve's buffers, constants and dt; with TMA (every solve
+// has tensor maps) its boxes are loaded through the solve's maps (tile_tma.cuh).  The scheme is a
 // template parameter: a run-time scheme switch inside one kernel holds all three flux
 // variants' registers at once and spills at the 64-register budget of 4 CTAs per SM.
 // One CTA per item rather than a persistent grid-stride loop: the hardware block
@@ -15,6 +16,7 @@
 #include <algorithm>
 
 #include "stage_tile.cuh"
+#include "tile_tma.cuh"
 
 namespace ausm {
 using namespace tile;
@@ -41,9 +43,8 @@ template <int SCHEME, int STAGE, bool EMIT>
 __global__ void __launch_bounds__(NT, AUSM_BATCH_MIN_BLOCKS)
     k_batch_stage(const BatchSolve* __restrict__ solves, const int s_lo, const int s_hi, const int t0, const int rot) {
   __shared__ float4 P[PH][PW];
-  __shared__ float2 Vs[(TY + 1) * (TX + 1)];
-  __shared__ float4 Fi[TY][TX + 1];
-  __shared__ float4 Fj[TY + 1][TX];
+  __shared__ float4 Ti[TY][TX + 1];
+  __shared__ float4 Tj[TY + 1][TX];
   const int tx = threadIdx.x, ty = threadIdx.y;
   const int item = t0 + blockIdx.x;
   const BatchSolve& d = solves[solve_of(solves, s_lo, s_hi, item)];
@@ -55,36 +56,56 @@ __global__ void __launch_bounds__(NT, AUSM_BATCH_MIN_BLOCKS)
   const float4* Qs = d.Q[STAGE <= 1 ? a : (STAGE == 2 ? b : c3)];
   const float4* Qn = d.Q[a];
   float4* Qo = d.Q[STAGE == 2 ? c3 : b];
-  const float2* V = d.V;
+  const float4* Mi = d.Mi;
+  const float4* Mj = d.Mj;
 
   const int ic = wrap_i(i0 + tx, M);
-  const float4 qa = tile_cell(Qs, V, c, M, N, ic, j0 + ty);
-  const float4 qb = tile_cell(Qs, V, c, M, N, ic, j0 + ty + 8);
+  const float4 qa = tile_cell(Qs, Mj, c, M, N, ic, j0 + ty);
+  const float4 qb = tile_cell(Qs, Mj, c, M, N, ic, j0 + ty + 8);
   int hr, hc;
   halo_entry(tx, ty, hr, hc);
   float4 qh = make_float4(1.0f, 0.0f, 0.0f, 1.0f);
-  if (hr >= 0) qh = tile_cell(Qs, V, c, M, N, wrap_i(i0 - 2 + hc, M), j0 - 2 + hr);
-  for (int r = ty; r <= TY; r += NWY) {
-    int j = j0 + r;
-    if (j <= N) {
-      Vs[r * (TX + 1) + tx] = __ldg(&V[(size_t)j * M + ic]);
-      if (tx == 0) Vs[r * (TX + 1) + TX] = __ldg(&V[(size_t)j * M + wrap_i(i0 + TX, M)]);
-    }
-  }
+  if (hr >= 0) qh = tile_cell(Qs, Mj, c, M, N, wrap_i(i0 - 2 + hc, M), j0 - 2 + hr);
+  stage_faces(Mi, Mj, Ti, Tj, i0, j0, ic, M, N, tx, ty);
   P[ty + 2][tx + 2] = to_prim<true>(qa, c.gm1);
   P[ty + 10][tx + 2] = to_prim<true>(qb, c.gm1);
   if (hr >= 0) P[hr][hc] = to_prim<true>(qh, c.gm1);
   __syncthreads();
 
-  faces_phase<SCHEME, TX + 1>(P, Vs, Fi, Fj, c, i0, j0, M, N, tx, ty);
+  const FaceW w = own_weights(Ti, Tj, tx, ty);
+  faces_phase<SCHEME>(P, Ti, Tj, c, i0, j0, M, N, tx, ty);
   __syncthreads();
 
   auto qn = [&](int h) { return __ldg(&Qn[(size_t)(j0 + ty + 8 * h) * M + i0 + tx]); };
-  uint32_t w = combine_phase<STAGE, EMIT, TX + 1>(Vs, Fi, Fj, qa, qb, qn, Qo, *d.dt, c, i0, j0, M, N, tx, ty);
+  uint32_t wv = combine_phase<STAGE, EMIT>(Ti, Tj, w, qa, qb, qn, Qo, *d.dt, c, i0, j0, M, N, tx, ty);
   if constexpr (EMIT) {
-    w = __reduce_max_sync(0xffffffffu, w);
-    if (tx == 0) atomicMax(d.wave, w);
+    wv = __reduce_max_sync(0xffffffffu, wv);
+    if (tx == 0) atomicMax(d.wave, wv);
   }
+}
+
+// TMA-staged form of k_batch_stage (stages 1-3): the tile's boxes come through the
+// solve's own tensor maps (in global memory).
+template <int SCHEME, int STAGE, bool EMIT>
+__global__ void __launch_bounds__(NT, AUSM_BATCH_MIN_BLOCKS)
+    k_batch_stage_tma(const BatchSolve* __restrict__ solves, const int s_lo, const int s_hi, const int t0,
+                      const int rot, int* __restrict__ err) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  unsigned char* smem = smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u);
+  const int item = t0 + blockIdx.x;
+  const BatchSolve& d = solves[solve_of(solves, s_lo, s_hi, item)];
+  const Consts c = d.c;
+  const int M = d.M, N = d.N;
+  const int local = item - d.tile0;
+  const int i0 = (local % d.tiles_x) * TX, j0 = (local / d.tiles_x) * TY;
+  const int a = (d.cur + rot) % 3, b = (a + 1) % 3, c3 = (a + 2) % 3;
+  const int s_in = STAGE == 1 ? a : (STAGE == 2 ? b : c3);
+  const CUtensorMap* mp = d.maps;
+  uint32_t wmax = 0u;
+  if (!tile_tma_body<SCHEME, STAGE, EMIT>(smem, &mp[s_in], &mp[3 + a], &mp[6], &mp[7], d.Q[s_in],
+                                          d.Q[STAGE == 2 ? c3 : b], d.Mi, d.Mj, *d.dt, c, M, N, i0, j0, err, wmax))
+    return;
+  if constexpr (EMIT) block_max_to(d.wave, wmax);
 }
 
 // dt = min(maxdt, cfl / max wave speed) per solve (ausm.js:457), then the wave-speed
@@ -167,26 +188,37 @@ void launch_batch_advance(BatchSolve* d, int nsolves, int steps, cudaStream_t s)
 
 namespace {
 template <int SC, int ST, bool E>
-void launch_b(const BatchSolve* d, int s_lo, int s_hi, int t_lo, int t_hi, int rot, cudaStream_t s) {
+void launch_b(const BatchSolve* d, int s_lo, int s_hi, int t_lo, int t_hi, int rot, int* err, cudaStream_t s) {
+  if constexpr (ST != 0) {
+    if (err) {
+      static bool attr = false;
+      if (!attr) {
+        cudaFuncSetAttribute(k_batch_stage_tma<SC, ST, E>, cudaFuncAttributeMaxDynamicSharedMemorySize, T1_SMEM);
+        attr = true;
+      }
+      k_batch_stage_tma<SC, ST, E><<<t_hi - t_lo, dim3(NWX, NWY), T1_SMEM, s>>>(d, s_lo, s_hi, t_lo, rot, err);
+      return;
+    }
+  }
   k_batch_stage<SC, ST, E><<<t_hi - t_lo, dim3(NWX, NWY), 0, s>>>(d, s_lo, s_hi, t_lo, rot);
 }
 template <int SC>
 void launch_scheme(int stage, bool emit, const BatchSolve* d, int s_lo, int s_hi, int t_lo, int t_hi, int rot,
-                   cudaStream_t s) {
-  if (stage == 0) launch_b<SC, 0, false>(d, s_lo, s_hi, t_lo, t_hi, rot, s);
-  else if (stage == 1) launch_b<SC, 1, false>(d, s_lo, s_hi, t_lo, t_hi, rot, s);
-  else if (stage == 2) launch_b<SC, 2, false>(d, s_lo, s_hi, t_lo, t_hi, rot, s);
-  else if (emit) launch_b<SC, 3, true>(d, s_lo, s_hi, t_lo, t_hi, rot, s);
-  else launch_b<SC, 3, false>(d, s_lo, s_hi, t_lo, t_hi, rot, s);
+                   int* err, cudaStream_t s) {
+  if (stage == 0) launch_b<SC, 0, false>(d, s_lo, s_hi, t_lo, t_hi, rot, nullptr, s);
+  else if (stage == 1) launch_b<SC, 1, false>(d, s_lo, s_hi, t_lo, t_hi, rot, err, s);
+  else if (stage == 2) launch_b<SC, 2, false>(d, s_lo, s_hi, t_lo, t_hi, rot, err, s);
+  else if (emit) launch_b<SC, 3, true>(d, s_lo, s_hi, t_lo, t_hi, rot, err, s);
+  else launch_b<SC, 3, false>(d, s_lo, s_hi, t_lo, t_hi, rot, err, s);
 }
 }  // namespace
 
 void launch_batch_stage(int scheme, int stage, bool emit, const BatchSolve* d, int s_lo, int s_hi, int t_lo,
-                        int t_hi, int rot, cudaStream_t s) {
+                        int t_hi, int rot, int* err, cudaStream_t s) {
   if (t_hi <= t_lo) return;
-  if (scheme == 0) launch_scheme<0>(stage, emit, d, s_lo, s_hi, t_lo, t_hi, rot, s);
-  else if (scheme == 1) launch_scheme<1>(stage, emit, d, s_lo, s_hi, t_lo, t_hi, rot, s);
-  else launch_scheme<2>(stage, emit, d, s_lo, s_hi, t_lo, t_hi, rot, s);
+  if (scheme == 0) launch_scheme<0>(stage, emit, d, s_lo, s_hi, t_lo, t_hi, rot, err, s);
+  else if (scheme == 1) launch_scheme<1>(stage, emit, d, s_lo, s_hi, t_lo, t_hi, rot, err, s);
+  else launch_scheme<2>(stage, emit, d, s_lo, s_hi, t_lo, t_hi, rot, err, s);
 }
 
 }  // namespace ausm

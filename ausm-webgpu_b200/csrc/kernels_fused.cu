@@ -8,31 +8,35 @@
 //   - P: primitives of the tile plus a 2-cell MUSCL halo on every side (corners
 //     unused), the periodic seam wrapped in i and the ghost rows (wall j=-1,-2, far
 //     field j=N,N+1) computed in place from the interior,
-//   - the (TX+1) x (TY+1) vertices of the tile,
-//   - Fi/Fj: flux x length of every i-face and j-face of the tile, each evaluated once
-//     (warp w takes face rows w and w+8 of each direction; warps 0 and 1 also the top
-//     face row and the right face column),
+//   - Ti/Tj: the FP64-computed face records of the tile's 33 x 16 i-faces and
+//     32 x 17 j-faces (normal, length, 1/A or the wave-speed factor), overwritten in
+//     place by the flux x length of each face, evaluated once (warp w takes face rows
+//     w and w+8 of each direction; warps 0 and 1 also the top face row and the right
+//     face column),
 // and each thread then assembles the residual and the stage combination of its two
 // cells and stores the new conserved states as float4.  The last stage-3 launch of a
 // step(n) call also reduces the new state's CFL wave speed (block max, one atomicMax
 // on the float bits, as cflReductionShaderCode ausm.js:535-581).
 //
-// k_fused_stage_tma (the default when M is even) is persistent: each CTA walks tiles
+// k_fused_stage_tma (the default) is persistent: each CTA walks tiles
 // t = blockIdx.x, blockIdx.x + gridDim.x, ... and stages them with TMA
 // (cp.async.bulk.tensor, no multicast) into a double buffer — the next tile's state
-// box (36 x 20 cells with halo) and vertex box load while the current tile computes,
-// and Qn for stages 2 and 3 loads during the face phase.  Out-of-range box columns
-// (the periodic seam) and rows (ghost rows) are filled in by the threads.  Every
-// mbarrier wait is bounded; on a timeout the CTA sets *err and stops.
-// k_fused_stage loads the same tile with per-thread loads (odd M, where the vertex row
-// pitch M*8 bytes is not a multiple of 16 and cannot be a TMA stride).
+// box (36 x 20 cells with halo) and face-record boxes load while the current tile
+// computes, and Qn for stages 2 and 3 loads during the face phase.  Out-of-range box
+// columns (the periodic seam) and rows (ghost rows) are filled in by the threads.
+// Every mbarrier wait is bounded; on a timeout the CTA sets *err and stops.
+// k_fused_stage loads the same tile with per-thread loads (AUSM_NO_TMA=1, and the
+// residual evaluation).
 //
-// HBM layout: interior state float4 [N][M] (row-major, no ghost rows), vertices
-// float2 [N+1][M].  Algorithmic traffic per cell and stage: 16 B state in, 16 B out,
-// 16 B Qn in (stages 2 and 3), 8 B vertex.
+// HBM layout: interior state float4 [N][M] (row-major, no ghost rows), face records
+// float4 Mi [N][M] and Mj [N+1][M].  Traffic per cell and stage: 16 B state in, 16 B
+// out, 16 B Qn in (stages 2 and 3), 32 B of face records.
+#include <cstdlib>
+#include <string>
+
 #include "ausm_internal.h"
 #include "stage_tile.cuh"
-#include "tma.cuh"
+#include "tile_tma.cuh"
 
 namespace ausm {
 
@@ -49,73 +53,62 @@ using namespace tile;
 template <int SCHEME, int STAGE, bool EMIT>
 __global__ void __launch_bounds__(NT, AUSM_FUSED_MIN_BLOCKS)
     k_fused_stage(const float4* __restrict__ Qs, const float4* __restrict__ Qn, float4* __restrict__ Qo,
-                  const float2* __restrict__ V, const float* __restrict__ dtp, uint32_t* __restrict__ wave,
-                  const Consts c, const int M, const int N) {
+                  const float4* __restrict__ Mi, const float4* __restrict__ Mj, const float* __restrict__ dtp,
+                  uint32_t* __restrict__ wave, const Consts c, const int M, const int N) {
   __shared__ float4 P[PH][PW];
-  __shared__ float2 Vs[(TY + 1) * (TX + 1)];
-  __shared__ float4 Fi[TY][TX + 1];
-  __shared__ float4 Fj[TY + 1][TX];
+  __shared__ float4 Ti[TY][TX + 1];
+  __shared__ float4 Tj[TY + 1][TX];
 
   const int tx = threadIdx.x, ty = threadIdx.y;
   const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY;
   const int ic = wrap_i(i0 + tx, M);  // column of the owned cells (wrapped when i0+tx >= M)
 
-  const float4 qa = tile_cell(Qs, V, c, M, N, ic, j0 + ty);
-  const float4 qb = tile_cell(Qs, V, c, M, N, ic, j0 + ty + 8);
+  const float4 qa = tile_cell(Qs, Mj, c, M, N, ic, j0 + ty);
+  const float4 qb = tile_cell(Qs, Mj, c, M, N, ic, j0 + ty + 8);
   int hr, hc;
   halo_entry(tx, ty, hr, hc);
   float4 qh = make_float4(1.0f, 0.0f, 0.0f, 1.0f);
-  if (hr >= 0) qh = tile_cell(Qs, V, c, M, N, wrap_i(i0 - 2 + hc, M), j0 - 2 + hr);
-  for (int r = ty; r <= TY; r += NWY) {  // vertices: rows ty, ty+8, ty+16; columns tx and TX
-    int j = j0 + r;
-    if (j <= N) {
-      Vs[r * (TX + 1) + tx] = __ldg(&V[(size_t)j * M + ic]);
-      if (tx == 0) Vs[r * (TX + 1) + TX] = __ldg(&V[(size_t)j * M + wrap_i(i0 + TX, M)]);
-    }
-  }
+  if (hr >= 0) qh = tile_cell(Qs, Mj, c, M, N, wrap_i(i0 - 2 + hc, M), j0 - 2 + hr);
+  stage_faces(Mi, Mj, Ti, Tj, i0, j0, ic, M, N, tx, ty);
   P[ty + 2][tx + 2] = to_prim<true>(qa, c.gm1);
   P[ty + 10][tx + 2] = to_prim<true>(qb, c.gm1);
   if (hr >= 0) P[hr][hc] = to_prim<true>(qh, c.gm1);
   __syncthreads();
 
-  faces_phase<SCHEME, TX + 1>(P, Vs, Fi, Fj, c, i0, j0, M, N, tx, ty);
+  const FaceW w = own_weights(Ti, Tj, tx, ty);
+  faces_phase<SCHEME>(P, Ti, Tj, c, i0, j0, M, N, tx, ty);
   __syncthreads();
 
   auto qn = [&](int h) { return __ldg(&Qn[(size_t)(j0 + ty + 8 * h) * M + i0 + tx]); };
-  uint32_t wmax = combine_phase<STAGE, EMIT, TX + 1>(Vs, Fi, Fj, qa, qb, qn, Qo, *dtp, c, i0, j0, M, N, tx, ty);
+  uint32_t wmax = combine_phase<STAGE, EMIT>(Ti, Tj, w, qa, qb, qn, Qo, *dtp, c, i0, j0, M, N, tx, ty);
   if constexpr (EMIT) block_max_to(wave, wmax);
 }
 
 // ---- persistent TMA-staged version ----
 namespace {
-// dynamic shared memory layout (offsets multiples of 128 B)
-constexpr int SQ_BYTES = PH * PW * 16;                 // 11520: state box (36 x 20 float4)
-constexpr int SV_BYTES = (TY + 1) * VW_TMA * 8;        // 4624:  vertex box (34 x 17 float2)
-constexpr int SN_BYTES = TY * TX * 16;                 // 8192:  Qn box (32 x 16 float4)
-constexpr int r128(int x) { return (x + 127) / 128 * 128; }
-constexpr int OFF_Q0 = 0, OFF_Q1 = OFF_Q0 + r128(SQ_BYTES);
-constexpr int OFF_V0 = OFF_Q1 + r128(SQ_BYTES), OFF_V1 = OFF_V0 + r128(SV_BYTES);
-constexpr int OFF_N = OFF_V1 + r128(SV_BYTES);
-constexpr int OFF_FI = OFF_N + r128(SN_BYTES);
-constexpr int OFF_FJ = OFF_FI + r128(TY * (TX + 1) * 16);
-constexpr int OFF_BAR = OFF_FJ + r128((TY + 1) * TX * 16);
+// dynamic shared memory layout of the persistent kernel (offsets multiples of 128 B);
+// buffers 0/1 alternate
+constexpr int BUF_BYTES = r128(SQ_BYTES) + r128(SI_BYTES) + r128(SJ_BYTES);
+constexpr int OFF_BUF0 = 0, OFF_BUF1 = BUF_BYTES;
+constexpr int OFF_I = r128(SQ_BYTES), OFF_J = OFF_I + r128(SI_BYTES);  // within a buffer
+constexpr int OFF_N = 2 * BUF_BYTES;
+constexpr int OFF_BAR = OFF_N + r128(SN_BYTES);
 constexpr int TMA_SMEM = OFF_BAR + 128 + 128;  // + alignment slack
 }  // namespace
 
 template <int SCHEME, int STAGE, bool EMIT>
 __global__ void __launch_bounds__(NT, AUSM_TMA_MIN_BLOCKS)
     k_fused_stage_tma(const __grid_constant__ TmaMapsLaunch tm, const float4* __restrict__ Qs,
-                      float4* __restrict__ Qo, const float2* __restrict__ V, const float* __restrict__ dtp,
-                      uint32_t* __restrict__ wave, int* __restrict__ err, const Consts c, const int M, const int N,
-                      const int tilesX, const int numTiles) {
+                      float4* __restrict__ Qo, const float4* __restrict__ Mi, const float4* __restrict__ Mj,
+                      const float* __restrict__ dtp, uint32_t* __restrict__ wave, int* __restrict__ err,
+                      const Consts c, const int M, const int N, const int tilesX, const int numTiles) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   // TMA destinations need 16-byte (we keep 128-byte) alignment of the dynamic region
   unsigned char* smem = smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u);
-  auto SQ = [&](int b) { return reinterpret_cast<float4(*)[PW]>(smem + OFF_Q0 + b * (OFF_Q1 - OFF_Q0)); };
-  auto SV = [&](int b) { return reinterpret_cast<float2*>(smem + OFF_V0 + b * (OFF_V1 - OFF_V0)); };
+  auto SQ = [&](int b) { return reinterpret_cast<float4(*)[PW]>(smem + b * BUF_BYTES); };
+  auto SI = [&](int b) { return reinterpret_cast<float4(*)[TX + 1]>(smem + b * BUF_BYTES + OFF_I); };
+  auto SJ = [&](int b) { return reinterpret_cast<float4(*)[TX]>(smem + b * BUF_BYTES + OFF_J); };
   float4(*SN)[TX] = reinterpret_cast<float4(*)[TX]>(smem + OFF_N);
-  float4(*Fi)[TX + 1] = reinterpret_cast<float4(*)[TX + 1]>(smem + OFF_FI);
-  float4(*Fj)[TX] = reinterpret_cast<float4(*)[TX]>(smem + OFF_FJ);
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem + OFF_BAR);  // [0],[1] tile buffers, [2] Qn
 
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * NWX + tx;
@@ -129,9 +122,10 @@ __global__ void __launch_bounds__(NT, AUSM_TMA_MIN_BLOCKS)
 
   auto issue_tile = [&](int t, int buf) {  // thread 0 only
     const int i0 = (t % tilesX) * TX, j0 = (t / tilesX) * TY;
-    mbar_expect_tx(&bars[buf], SQ_BYTES + SV_BYTES);
+    mbar_expect_tx(&bars[buf], SQ_BYTES + SI_BYTES + SJ_BYTES);
     tma_load_2d(SQ(buf), &tm.qs, 4 * (i0 - 2), j0 - 2, &bars[buf]);
-    tma_load_2d(SV(buf), &tm.v, 2 * i0, j0, &bars[buf]);
+    tma_load_2d(SI(buf), &tm.mi, 4 * i0, j0, &bars[buf]);
+    tma_load_2d(SJ(buf), &tm.mj, 4 * i0, j0, &bars[buf]);
   };
 
   const float dt = *dtp;
@@ -170,27 +164,24 @@ __global__ void __launch_bounds__(NT, AUSM_TMA_MIN_BLOCKS)
       phase ^= 1u << b;
     }
     float4(*P)[PW] = SQ(b);
-    float2* Vs = SV(b);
+    float4(*Ti)[TX + 1] = SI(b);
+    float4(*Tj)[TX] = SJ(b);
     // owned cells and the halo entry: fill seam columns and ghost rows, keep the owned
     // conserved states, convert to primitives in place
     auto stage_entry = [&](int pr, int pc) {
       const int ig = i0 - 2 + pc, j = j0 - 2 + pr;
       float4 q;
       if (j >= 0 && j < N) q = (ig >= 0 && ig < M) ? P[pr][pc] : __ldg(&Qs[(size_t)j * M + wrap_i(ig, M)]);
-      else q = tile_cell(Qs, V, c, M, N, wrap_i(ig, M), j);
+      else q = tile_cell(Qs, Mj, c, M, N, wrap_i(ig, M), j);
       P[pr][pc] = to_prim<true>(q, c.gm1);
       return q;
     };
     const float4 qa = stage_entry(ty + 2, tx + 2);
     const float4 qb = stage_entry(ty + 10, tx + 2);
     if (hr >= 0) stage_entry(hr, hc);
-    if (i0 + TX + 1 >= M) {  // vertex columns past the seam
-      for (int r = ty; r <= TY; r += NWY) {
-        const int j = j0 + r;
-        if (j > N) continue;
-        if (i0 + tx >= M) Vs[r * VW_TMA + tx] = __ldg(&V[(size_t)j * M + wrap_i(i0 + tx, M)]);
-        if (tx < 2 && i0 + TX + tx >= M) Vs[r * VW_TMA + TX + tx] = __ldg(&V[(size_t)j * M + wrap_i(i0 + TX + tx, M)]);
-      }
+    if (i0 + TX >= M && tx == 0) {  // the face column past the seam (zero-filled by the box)
+      for (int r = ty; r < TY; r += NWY)
+        if (j0 + r < N) Ti[r][M - i0] = __ldg(&Mi[(size_t)(j0 + r) * M]);
     }
     __syncthreads();
     // ---- prefetch the next tile into the other buffer (free since the last barrier) ----
@@ -199,7 +190,8 @@ __global__ void __launch_bounds__(NT, AUSM_TMA_MIN_BLOCKS)
       issue_tile(t + gridDim.x, b ^ 1);
       pending |= 1u << (b ^ 1);
     }
-    faces_phase<SCHEME, VW_TMA>(P, Vs, Fi, Fj, c, i0, j0, M, N, tx, ty);
+    const FaceW w = own_weights(Ti, Tj, tx, ty);
+    faces_phase<SCHEME>(P, Ti, Tj, c, i0, j0, M, N, tx, ty);
     __syncthreads();
     if constexpr (STAGE >= 2) {
       bool okn = mbar_wait(&bars[2], k & 1);
@@ -213,8 +205,8 @@ __global__ void __launch_bounds__(NT, AUSM_TMA_MIN_BLOCKS)
       }
     }
     auto qn = [&](int h) { return SN[ty + 8 * h][tx]; };
-    wmax = max(wmax, combine_phase<STAGE, EMIT, VW_TMA>(Vs, Fi, Fj, qa, qb, qn, Qo, dt, c, i0, j0, M, N, tx, ty));
-    __syncthreads();  // Fi, Fj, SN and buffer b are free for reuse
+    wmax = max(wmax, combine_phase<STAGE, EMIT>(Ti, Tj, w, qa, qb, qn, Qo, dt, c, i0, j0, M, N, tx, ty));
+    __syncthreads();  // SN and buffer b are free for reuse
   }
   if (failed) {
     if (tid == 0) {
@@ -227,13 +219,41 @@ __global__ void __launch_bounds__(NT, AUSM_TMA_MIN_BLOCKS)
   if constexpr (EMIT) block_max_to(wave, wmax);
 }
 
+// ---- TMA-staged, one tile per CTA (the default) ----
+template <int SCHEME, int STAGE, bool EMIT>
+__global__ void __launch_bounds__(NT, AUSM_FUSED_MIN_BLOCKS)
+    k_fused_tile_tma(const __grid_constant__ TmaMapsLaunch tm, const float4* __restrict__ Qs,
+                     float4* __restrict__ Qo, const float4* __restrict__ Mi, const float4* __restrict__ Mj,
+                     const float* __restrict__ dtp, uint32_t* __restrict__ wave, int* __restrict__ err,
+                     const Consts c, const int M, const int N) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  unsigned char* smem = smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u);
+  uint32_t wmax = 0u;
+  if (!tile_tma_body<SCHEME, STAGE, EMIT>(smem, &tm.qs, &tm.qn, &tm.mi, &tm.mj, Qs, Qo, Mi, Mj, *dtp, c, M, N,
+                                          blockIdx.x * TX, blockIdx.y * TY, err, wmax))
+    return;
+  if constexpr (EMIT) block_max_to(wave, wmax);
+}
+
 // ---- launchers ----
 namespace {
 template <int S, int ST, bool E>
-void launch_t(const float4* Qs, const float4* Qn, float4* Qo, const float2* V, const float* dt, uint32_t* wave,
-              const Consts& c, int M, int N, const TmaMapsLaunch* tm, int* err, cudaStream_t s) {
+void launch_t(const float4* Qs, const float4* Qn, float4* Qo, const float4* Mi, const float4* Mj, const float* dt,
+              uint32_t* wave, const Consts& c, int M, int N, const TmaMapsLaunch* tm, int* err, cudaStream_t s) {
   const int tilesX = (M + TX - 1) / TX, tilesY = (N + TY - 1) / TY;
-  if (tm && ST != 0) {
+  static const bool per_tile = [] {
+    const char* e = std::getenv("AUSM_TMA_MODE");  // "tile" or "persistent" (A/B timing)
+    return !(e && std::string(e) == "persistent");
+  }();
+  if (tm && ST != 0 && per_tile) {
+    auto kern = k_fused_tile_tma<S, ST, E>;
+    static bool attr = false;
+    if (!attr) {
+      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, T1_SMEM);
+      attr = true;
+    }
+    kern<<<dim3(tilesX, tilesY), dim3(NWX, NWY), T1_SMEM, s>>>(*tm, Qs, Qo, Mi, Mj, dt, wave, err, c, M, N);
+  } else if (tm && ST != 0) {
     static int blocks_per_sm = 0, sms = 0;
     auto kern = k_fused_stage_tma<S, ST, E>;
     if (!blocks_per_sm) {
@@ -246,42 +266,43 @@ void launch_t(const float4* Qs, const float4* Qn, float4* Qo, const float2* V, c
     }
     const int numTiles = tilesX * tilesY;
     const int grid = std::min(numTiles, blocks_per_sm * sms);
-    kern<<<grid, dim3(NWX, NWY), TMA_SMEM, s>>>(*tm, Qs, Qo, V, dt, wave, err, c, M, N, tilesX, numTiles);
+    kern<<<grid, dim3(NWX, NWY), TMA_SMEM, s>>>(*tm, Qs, Qo, Mi, Mj, dt, wave, err, c, M, N, tilesX, numTiles);
   } else {
-    k_fused_stage<S, ST, E><<<dim3(tilesX, tilesY), dim3(NWX, NWY), 0, s>>>(Qs, Qn, Qo, V, dt, wave, c, M, N);
+    k_fused_stage<S, ST, E><<<dim3(tilesX, tilesY), dim3(NWX, NWY), 0, s>>>(Qs, Qn, Qo, Mi, Mj, dt, wave, c, M, N);
   }
 }
 template <int S>
-void launch_s(int stage, bool emit, const float4* Qs, const float4* Qn, float4* Qo, const float2* V,
-              const float* dt, uint32_t* wave, const Consts& c, int M, int N, const TmaMapsLaunch* tm, int* err,
-              cudaStream_t s) {
+void launch_s(int stage, bool emit, const float4* Qs, const float4* Qn, float4* Qo, const float4* Mi,
+              const float4* Mj, const float* dt, uint32_t* wave, const Consts& c, int M, int N,
+              const TmaMapsLaunch* tm, int* err, cudaStream_t s) {
   switch (stage) {
-    case 0: launch_t<S, 0, false>(Qs, Qn, Qo, V, dt, wave, c, M, N, tm, err, s); break;
-    case 1: launch_t<S, 1, false>(Qs, Qn, Qo, V, dt, wave, c, M, N, tm, err, s); break;
-    case 2: launch_t<S, 2, false>(Qs, Qn, Qo, V, dt, wave, c, M, N, tm, err, s); break;
+    case 0: launch_t<S, 0, false>(Qs, Qn, Qo, Mi, Mj, dt, wave, c, M, N, tm, err, s); break;
+    case 1: launch_t<S, 1, false>(Qs, Qn, Qo, Mi, Mj, dt, wave, c, M, N, tm, err, s); break;
+    case 2: launch_t<S, 2, false>(Qs, Qn, Qo, Mi, Mj, dt, wave, c, M, N, tm, err, s); break;
     default:
-      if (emit) launch_t<S, 3, true>(Qs, Qn, Qo, V, dt, wave, c, M, N, tm, err, s);
-      else launch_t<S, 3, false>(Qs, Qn, Qo, V, dt, wave, c, M, N, tm, err, s);
+      if (emit) launch_t<S, 3, true>(Qs, Qn, Qo, Mi, Mj, dt, wave, c, M, N, tm, err, s);
+      else launch_t<S, 3, false>(Qs, Qn, Qo, Mi, Mj, dt, wave, c, M, N, tm, err, s);
   }
 }
 }  // namespace
 
 void launch_fused_stage(int scheme, int stage, bool emit, const float4* Qs, const float4* Qn, float4* Qo,
-                        const float2* V, const float* dt, uint32_t* wave, const Consts& c, int M, int N,
-                        const TmaMapsLaunch* tm, int* err, cudaStream_t s) {
+                        const float4* Mi, const float4* Mj, const float* dt, uint32_t* wave, const Consts& c, int M,
+                        int N, const TmaMapsLaunch* tm, int* err, cudaStream_t s) {
   switch (scheme) {
-    case 0: launch_s<0>(stage, emit, Qs, Qn, Qo, V, dt, wave, c, M, N, tm, err, s); break;
-    case 1: launch_s<1>(stage, emit, Qs, Qn, Qo, V, dt, wave, c, M, N, tm, err, s); break;
-    default: launch_s<2>(stage, emit, Qs, Qn, Qo, V, dt, wave, c, M, N, tm, err, s); break;
+    case 0: launch_s<0>(stage, emit, Qs, Qn, Qo, Mi, Mj, dt, wave, c, M, N, tm, err, s); break;
+    case 1: launch_s<1>(stage, emit, Qs, Qn, Qo, Mi, Mj, dt, wave, c, M, N, tm, err, s); break;
+    default: launch_s<2>(stage, emit, Qs, Qn, Qo, Mi, Mj, dt, wave, c, M, N, tm, err, s); break;
   }
 }
 
 // Tensor maps of the TMA kernel: state buffers as 2-D float tensors of 4M x N
-// (row pitch 16 M bytes) with the halo box 144 x 20 and the Qn box 128 x 16, vertices
-// as 2M x (N+1) (pitch 8 M bytes, needs M even) with the box 68 x 17.
-bool encode_tma_maps(const float4* const Q[3], const float2* V, int M, int N, TmaMaps* out) {
+// (row pitch 16 M bytes) with the halo box 144 x 20 and the Qn box 128 x 16; face
+// records Mi as 4M x N with the box 132 x 16, Mj as 4M x (N+1) with the box 128 x 17.
+// Every box's row is a multiple of 16 bytes and every x coordinate a multiple of 4
+// floats (16 bytes).
+bool encode_tma_maps(const float4* const Q[3], const float4* Mi, const float4* Mj, int M, int N, TmaMaps* out) {
   out->ok = false;
-  if (M % 2 != 0) return false;
   using Encode = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
                               const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
                               CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
@@ -308,36 +329,29 @@ bool encode_tma_maps(const float4* const Q[3], const float2* V, int M, int N, Tm
     if (!enc(&out->halo[b], Q[b], 4ull * M, N, 16ull * M, 4 * PW, PH)) return false;
     if (!enc(&out->plain[b], Q[b], 4ull * M, N, 16ull * M, 4 * TX, TY)) return false;
   }
-  if (!enc(&out->v, V, 2ull * M, N + 1, 8ull * M, 2 * VW_TMA, TY + 1)) return false;
+  if (!enc(&out->mi, Mi, 4ull * M, N, 16ull * M, 4 * (TX + 1), TY)) return false;
+  if (!enc(&out->mj, Mj, 4ull * M, N + 1, 16ull * M, 4 * TX, TY + 1)) return false;
   out->ok = true;
   return true;
 }
 
-// Wave speed + max of an interior state with metrics recomputed from the vertices
-// (seeds dt after init_state / set_state, main.js:649-652).
-__global__ void k_wave_interior(const float4* __restrict__ Q, const float2* __restrict__ V, float gamma, int M, int N,
+// Wave speed + max of an interior state from the cells' wave-speed factors (seeds dt
+// after init_state / set_state, main.js:649-652).
+__global__ void k_wave_interior(const float4* __restrict__ Q, const float4* __restrict__ Mj, float gamma, int M, int N,
                                 uint32_t* wave) {
   uint32_t wm = 0u;
   size_t total = (size_t)M * N;
   for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < total; k += (size_t)gridDim.x * blockDim.x) {
-    int j = (int)(k / M), i = (int)(k - (size_t)j * M);
-    int r = (i + 1) % M;
-    float2 a = V[(size_t)j * M + i], b = V[(size_t)j * M + r], cv = V[(size_t)(j + 1) * M + i],
-           d = V[(size_t)(j + 1) * M + r];
-    float ll = sqrtf((a.x - cv.x) * (a.x - cv.x) + (a.y - cv.y) * (a.y - cv.y));
-    float lr = sqrtf((b.x - d.x) * (b.x - d.x) + (b.y - d.y) * (b.y - d.y));
-    float lu = sqrtf((cv.x - d.x) * (cv.x - d.x) + (cv.y - d.y) * (cv.y - d.y));
-    float ld = sqrtf((a.x - b.x) * (a.x - b.x) + (a.y - b.y) * (a.y - b.y));
-    float w = wave_speed<false>(Q[k], ((ll + lr) + lu) + ld, quad_area(a, b, cv, d), gamma);
+    float w = wave_speed_w<false>(Q[k], Mj[k].w, gamma);
     wm = max(wm, __float_as_uint(w));
   }
   block_max_to(wave, wm);
 }
 
-void launch_wave_interior(const float4* Q, const float2* V, float gamma, int M, int N, uint32_t* wave,
+void launch_wave_interior(const float4* Q, const float4* Mj, float gamma, int M, int N, uint32_t* wave,
                           cudaStream_t s) {
   int blocks = (int)std::min<size_t>(((size_t)M * N + 255) / 256, 148 * 8);
-  k_wave_interior<<<blocks, 256, 0, s>>>(Q, V, gamma, M, N, wave);
+  k_wave_interior<<<blocks, 256, 0, s>>>(Q, Mj, gamma, M, N, wave);
 }
 
 }  // namespace ausm

@@ -100,17 +100,109 @@ __global__ void k_grid_multicolor(float2* __restrict__ V, int M, int N, int colo
   block_max_to(move, mv);
 }
 
+// ---- FP64 grid (multicolor TTM generator of the fused engine) and FP64 metrics ----
+__global__ void k_grid_init_d(double2* __restrict__ V, int M, int N, double first_spacing) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
+  if (i >= M || j > N || j == 0 || j == N) return;
+  double2 a = V[i], b = V[(size_t)N * M + i];
+  double t;
+  if (first_spacing <= 0.0) {
+    t = (double)j / (double)N;
+  } else {
+    double L = sqrt((b.x - a.x) * (b.x - a.x) + (b.y - a.y) * (b.y - a.y));
+    double h = first_spacing / L;
+    double lo = 1.0 + 1e-12, hi = 2.0;
+    if (h * N >= 1.0) { lo = 1e-6; hi = 1.0 - 1e-12; }
+    for (int it = 0; it < 200; it++) {
+      double q = 0.5 * (lo + hi);
+      double s = h * (pow(q, (double)N) - 1.0) / (q - 1.0);
+      if ((s > 1.0) == (h * N < 1.0)) hi = q; else lo = q;
+    }
+    double q = 0.5 * (lo + hi);
+    t = h * (pow(q, (double)j) - 1.0) / (q - 1.0);
+  }
+  V[(size_t)j * M + i] = make_double2(a.x * (1.0 - t) + b.x * t, a.y * (1.0 - t) + b.y * t);
+}
+
+__device__ __forceinline__ double2 ttm_point_d(const double2* __restrict__ s, int M, int i, int j, double omega) {
+  int l = i == 0 ? M - 1 : i - 1, r = i == M - 1 ? 0 : i + 1;
+  size_t rj = (size_t)j * M, ru = (size_t)(j + 1) * M, rd = (size_t)(j - 1) * M;
+  double2 c = s[rj + i], L = s[rj + l], R = s[rj + r], D = s[rd + i], U = s[ru + i];
+  double2 DL = s[rd + l], DR = s[rd + r], UL = s[ru + l], UR = s[ru + r];
+  double xix = 0.5 * (R.x - L.x), xiy = 0.5 * (R.y - L.y);
+  double etx = 0.5 * (U.x - D.x), ety = 0.5 * (U.y - D.y);
+  double xex = 0.25 * (UR.x + DL.x - UL.x - DR.x), xey = 0.25 * (UR.y + DL.y - UL.y - DR.y);
+  double alpha = etx * etx + ety * ety, gam = xix * xix + xiy * xiy, beta = xix * etx + xiy * ety;
+  double den = 2.0 * (alpha + gam);
+  double npx = (alpha * (L.x + R.x) + gam * (D.x + U.x) - 2.0 * beta * xex) / den;
+  double npy = (alpha * (L.y + R.y) + gam * (D.y + U.y) - 2.0 * beta * xey) / den;
+  double jac = xix * ety - xiy * etx;
+  if (jac < 0.0) return make_double2(c.x * (1.0 - omega) + npx * omega, c.y * (1.0 - omega) + npy * omega);
+  return c;
+}
+// One colour of the FP64 multicolour sweep (colouring as k_grid_multicolor).
+__global__ void k_grid_multicolor_d(double2* __restrict__ V, int M, int N, int color, double omega, uint32_t* move) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
+  uint32_t mv = 0u;
+  if (i < M && j >= 1 && j < N) {
+    int col = ((M & 1) && i == M - 1) ? 4 + (j & 1) : (i & 1) * 2 + (j & 1);
+    if (col == color) {
+      double2 p = ttm_point_d(V, M, i, j, omega);
+      double2 o = V[(size_t)j * M + i];
+      mv = __float_as_uint((float)fmax(fabs(p.x - o.x), fabs(p.y - o.y)));
+      V[(size_t)j * M + i] = p;
+    }
+  }
+  block_max_to(move, mv);
+}
+__global__ void k_d2f(const double2* __restrict__ a, float2* __restrict__ b, size_t n) {
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x)
+    b[k] = make_float2((float)a[k].x, (float)a[k].y);
+}
+__global__ void k_f2d(const float2* __restrict__ a, double2* __restrict__ b, size_t n) {
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x)
+    b[k] = make_double2(a[k].x, a[k].y);
+}
+
+// Face records in FP64, rounded once to FP32 (shaders/grid.js:115-147 computes them in
+// FP32 from FP32 vertices).  Mi[j][i]: face between cells (i-1, j) and (i, j), tangent
+// V(i, j+1) - V(i, j), unit normal (-t.y, t.x), its length, and 1 / area of cell
+// (i, j).  Mj[j][i], j = 0..N: face between cells (i, j-1) and (i, j), tangent
+// V(i, j) - V(i+1, j), normal, length, and for j < N the wave-speed factor
+// (l_l + l_r + l_u + l_d) / (2 A) of cell (i, j) (ausm.js:617-630).
+__global__ void k_metrics_d(const double2* __restrict__ V, float4* __restrict__ Mi, float4* __restrict__ Mj, int M,
+                            int N) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
+  if (i >= M || j > N) return;
+  const int r = i + 1 == M ? 0 : i + 1;
+  const double2 a = V[(size_t)j * M + i], b = V[(size_t)j * M + r];
+  double tx = a.x - b.x, ty = a.y - b.y;
+  double ld = sqrt(tx * tx + ty * ty);
+  float w = 0.0f;
+  if (j < N) {
+    const double2 c = V[(size_t)(j + 1) * M + i], d = V[(size_t)(j + 1) * M + r];
+    double ux = c.x - a.x, uy = c.y - a.y;
+    double ll = sqrt(ux * ux + uy * uy);
+    double lr = sqrt((d.x - b.x) * (d.x - b.x) + (d.y - b.y) * (d.y - b.y));
+    double lu = sqrt((c.x - d.x) * (c.x - d.x) + (c.y - d.y) * (c.y - d.y));
+    double A = 0.5 * fabs((d.x - a.x) * (c.y - b.y) - (c.x - b.x) * (d.y - a.y));
+    w = (float)((ll + lr + lu + ld) / (2.0 * A));
+    Mi[(size_t)j * M + i] = make_float4((float)(-uy / ll), (float)(ux / ll), (float)ll, (float)(1.0 / A));
+  }
+  Mj[(size_t)j * M + i] = make_float4((float)(-ty / ld), (float)(tx / ld), (float)ld, w);
+}
+
 // ---- surface force (graphs.js:186-272): FP32 pressure of the first interior cell,
 // FP64 face length, normal and sum; also Cp per wall face ----
-__global__ void k_forces(const float4* __restrict__ row0, const float2* __restrict__ V, const Consts c, int M,
+__global__ void k_forces(const float4* __restrict__ row0, const double2* __restrict__ V, const Consts c, int M,
                          double* parts, double* cp, double q_inf, double p_inf) {
   double fx = 0.0, fy = 0.0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < M; i += gridDim.x * blockDim.x) {
     float4 s = row0[i];
     float rho = s.x, u = s.y / rho, v = s.z / rho;
     float p = (s.w - 0.5f * rho * (u * u + v * v)) * (c.gamma - 1.0f);
-    float2 a = V[i], b = V[(i + 1) % M];
-    double dx = (double)b.x - a.x, dy = (double)b.y - a.y;
+    double2 a = V[i], b = V[(i + 1) % M];
+    double dx = b.x - a.x, dy = b.y - a.y;
     double len = sqrt(dx * dx + dy * dy);
     double nx = dy / len, ny = -dx / len;  // (vtx2.y - vtx1.y, vtx1.x - vtx2.x) / length
     fx += -(double)p * len * nx;
@@ -203,7 +295,7 @@ void launch_grid_jacobi(const float2* src, float2* dst, int M, int N, cudaStream
 void launch_grid_multicolor(float2* V, int M, int N, int color, float omega, uint32_t* move, cudaStream_t s) {
   k_grid_multicolor<<<grid16(M, N + 1), B16, 0, s>>>(V, M, N, color, omega, move);
 }
-void launch_forces(const float4* row0, const float2* V, const Consts& c, int M, double* acc, double* parts,
+void launch_forces(const float4* row0, const double2* V, const Consts& c, int M, double* acc, double* parts,
                    double* cp, double q_inf, double p_inf, cudaStream_t s) {
   int blocks = std::min((M + 255) / 256, 148);
   k_forces<<<blocks, 256, 0, s>>>(row0, V, c, M, parts, cp, q_inf, p_inf);
@@ -213,6 +305,17 @@ void launch_sumsq_rho(const float4* R, size_t n, double* acc, double* parts, cud
   const int blocks = grid1d(n);  // <= kMaxParts
   k_sumsq_rho<<<blocks, 256, 0, s>>>(R, n, parts);
   k_sum_parts<<<1, 256, 0, s>>>(parts, blocks, acc);
+}
+void launch_grid_init_d(double2* V, int M, int N, double first_spacing, cudaStream_t s) {
+  k_grid_init_d<<<grid16(M, N + 1), B16, 0, s>>>(V, M, N, first_spacing);
+}
+void launch_grid_multicolor_d(double2* V, int M, int N, int color, double omega, uint32_t* move, cudaStream_t s) {
+  k_grid_multicolor_d<<<grid16(M, N + 1), B16, 0, s>>>(V, M, N, color, omega, move);
+}
+void launch_d2f(const double2* a, float2* b, size_t n, cudaStream_t s) { k_d2f<<<grid1d(n), 256, 0, s>>>(a, b, n); }
+void launch_f2d(const float2* a, double2* b, size_t n, cudaStream_t s) { k_f2d<<<grid1d(n), 256, 0, s>>>(a, b, n); }
+void launch_metrics_d(const double2* V, float4* Mi, float4* Mj, int M, int N, cudaStream_t s) {
+  k_metrics_d<<<grid16(M, N + 1), B16, 0, s>>>(V, Mi, Mj, M, N);
 }
 void launch_field(const float4* Qint, const float2* V, const Consts& c, int kind, int M, int N, float* out,
                   cudaStream_t s) {

@@ -88,23 +88,25 @@ template <bool FAST> __device__ __forceinline__ float4 to_prim(float4 Q, float g
 }
 
 // Wall ghost (ausm.js:57-64): velocity of the first interior cell reflected about the
-// wall normal of the face between vertices a=(i,0), b=(i+1,0); rho and rhoE kept.
-template <bool FAST> __device__ __forceinline__ float4 wall_ghost(float4 s, float2 a, float2 b) {
-  float nx, ny, len;
-  edge_normal<FAST>(a, b, nx, ny, len);
+// wall normal (nx, ny); rho and rhoE kept.
+template <bool FAST> __device__ __forceinline__ float4 wall_ghost_n(float4 s, float nx, float ny) {
   float rho = s.x;
   float u = fdiv<FAST>(s.y, rho), v = fdiv<FAST>(s.z, rho);
   float dn = 2.0f * (nx * u + ny * v);
   float gu = u - dn * nx, gv = v - dn * ny;
   return make_float4(rho, gu * rho, gv * rho, s.w);
 }
-
-// Far-field ghosts (ausm.js:65-117) from the last interior cell s and the outer face
-// between vertices a=(i,N), b=(i+1,N).  g1 = row N+1, g2 = row N+2.
-template <bool FAST>
-__device__ __forceinline__ void far_ghosts(float4 s, float2 a, float2 b, const Consts& c, float4& g1, float4& g2) {
+// ... with the normal of the wall face between vertices a=(i,0), b=(i+1,0)
+template <bool FAST> __device__ __forceinline__ float4 wall_ghost(float4 s, float2 a, float2 b) {
   float nx, ny, len;
   edge_normal<FAST>(a, b, nx, ny, len);
+  return wall_ghost_n<FAST>(s, nx, ny);
+}
+
+// Far-field ghosts (ausm.js:65-117) from the last interior cell s and the unit normal
+// (nx, ny) of the outer face.  g1 = row N+1, g2 = row N+2.
+template <bool FAST>
+__device__ __forceinline__ void far_ghosts_n(float4 s, float nx, float ny, const Consts& c, float4& g1, float4& g2) {
   float rho = s.x;
   float u = fdiv<FAST>(s.y, rho), v = fdiv<FAST>(s.z, rho);
   float inout = nx * c.inflow.x + ny * c.inflow.y;
@@ -138,6 +140,13 @@ __device__ __forceinline__ void far_ghosts(float4 s, float2 a, float2 b, const C
     g1 = s;
   }
   g2 = make_float4(2.0f * g1.x - s.x, 2.0f * g1.y - s.y, 2.0f * g1.z - s.z, 2.0f * g1.w - s.w);
+}
+// ... with the normal of the outer face between vertices a=(i,N), b=(i+1,N)
+template <bool FAST>
+__device__ __forceinline__ void far_ghosts(float4 s, float2 a, float2 b, const Consts& c, float4& g1, float4& g2) {
+  float nx, ny, len;
+  edge_normal<FAST>(a, b, nx, ny, len);
+  far_ghosts_n<FAST>(s, nx, ny, c, g1, g2);
 }
 
 // van Albada-limited MUSCL on two primitive components at once (packed f32x2), the
@@ -311,6 +320,17 @@ template <bool FAST> __device__ __forceinline__ float wave_speed(float4 s, float
   float a = fsqrt<FAST>(gamma * T);
   float speed = fsqrt<FAST>(u * u + v * v);
   return fdiv<FAST>((speed + a) * lsum, 2.0f * area);
+}
+
+// ... with the cell's precomputed factor W = sum(l) / (2 A)
+template <bool FAST> __device__ __forceinline__ float wave_speed_w(float4 s, float W, float gamma) {
+  float rho = s.x;
+  float u = fdiv<FAST>(s.y, rho), v = fdiv<FAST>(s.z, rho);
+  float p = (s.w - 0.5f * rho * (u * u + v * v)) * (gamma - 1.0f);
+  float T = fdiv<FAST>(p, rho);
+  float a = fsqrt<FAST>(gamma * T);
+  float speed = fsqrt<FAST>(u * u + v * v);
+  return (speed + a) * W;
 }
 
 // Cell area of the quad a=(i,j), b=(i+1,j), c=(i,j+1), d=(i+1,j+1) (shaders/grid.js:140).

@@ -91,12 +91,13 @@ std::string validate(const AusmRequest& r) {
   return "";
 }
 
-// Device bytes of a fused-engine solver driven by the server: vertices, three state
-// buffers, the Cp array, and a fixed 64 KiB for the per-solver scalars and the
+// Device bytes of a fused-engine solver driven by the server: FP32 and FP64 vertices
+// (8 + 16 per vertex), the two face-record arrays (16 per face), three state buffers
+// (48 per cell), the Cp array, and a fixed 64 KiB for the per-solver scalars and the
 // reduction scratch (2 x 2368 doubles), allocation rounding included.
 double request_bytes(const AusmRequest& r) {
   const double M = r.M, N = r.N;
-  return 8.0 * M * (N + 1) + 3.0 * 16.0 * M * N + 8.0 * M + 65536.0;
+  return 40.0 * M * (N + 1) + 16.0 * M * N + 48.0 * M * N + 8.0 * M + 65536.0;
 }
 
 }  // namespace

@@ -19,8 +19,11 @@ struct ausm_solver {
   std::vector<double> body, outer;  // M x 2
   bool has_body = false, has_outer = false, has_grid = false, has_state = false;
   double stretch = 0.0;
-  float2* V = nullptr;
-  float2* V2 = nullptr;
+  float2* V = nullptr;    // vertices, FP32 (reference layout, API, reference engine)
+  float2* V2 = nullptr;   // Jacobi ping-pong
+  double2* Vd = nullptr;  // vertices, FP64 (multicolor generator, metrics, forces)
+  float4* Mi = nullptr;   // FP64-computed face records, i-faces [N][M]
+  float4* Mj = nullptr;   // ... j-faces [N+1][M]
   float4* Q[3] = {nullptr, nullptr, nullptr};
   int cur = 0;
   float4* S[3] = {nullptr, nullptr, nullptr};

@@ -1,8 +1,16 @@
 // Tile compute shared by the single-solve and batched stage kernels: tile geometry,
 // staging of a tile's cells (interior loads, seam wrap, ghost rows), the face phase
 // (flux x length of every face of the tile, each once) and the combine phase (residual
-// and RK stage combination of the two cells a thread owns).  See kernels_fused.cu for
-// the work decomposition.
+// and RK stage combination of the two cells a thread owns).
+//
+// Geometry comes from the FP64-computed face records (k_metrics_d): Mi[j][i] =
+// (nx, ny, len, 1/A) of the face left of cell (i, j), Mj[j][i] = (nx, ny, len, W) of
+// the face below it, W the cell's wave-speed factor.  A tile stages the records of its
+// faces in shared memory (Ti: 16 rows x 33 faces, Tj: 17 rows x 32 faces); the face
+// phase reads a face's record and overwrites it with that face's flux x length, so the
+// flux tiles share that memory.  Each face is read and written by one thread only, and
+// the thread that owns a cell computes that cell's left and lower faces, so it keeps
+// the cell's 1/A and W in registers (FaceW) before the records are overwritten.
 #pragma once
 #include "ausm_internal.h"
 
@@ -10,7 +18,6 @@ namespace ausm {
 namespace tile {
 constexpr int TX = 32, TY = 16, NWX = 32, NWY = 8, NT = NWX * NWY;
 constexpr int PW = TX + 4, PH = TY + 4;
-constexpr int VW_TMA = TX + 2;  // vertex box width: 34 x 8 B = 272 B, a multiple of 16 B
 
 // i in [-2, M + TX + 2) -> [0, M); the last branch only runs for M < TX + 3
 __device__ __forceinline__ int wrap_i(int i, int M) {
@@ -21,17 +28,20 @@ __device__ __forceinline__ int wrap_i(int i, int M) {
 }
 
 // Conserved state of tile cell (i, j) with j in [-2, N+1]: interior cells are loaded,
-// ghost rows are computed from the adjacent interior row (boundary pass ausm.js:34-120,
-// loadState clamp ausm.js:141 maps j = -1 and -2 to the wall ghost).
-__device__ __forceinline__ float4 tile_cell(const float4* __restrict__ Qs, const float2* __restrict__ V,
+// ghost rows are computed from the adjacent interior row and the wall / outer face
+// normal (boundary pass ausm.js:34-120, loadState clamp ausm.js:141 maps j = -1 and -2
+// to the wall ghost).
+__device__ __forceinline__ float4 tile_cell(const float4* __restrict__ Qs, const float4* __restrict__ Mj,
                                             const Consts& c, int M, int N, int i, int j) {
   if (j >= 0 && j < N) return __ldg(&Qs[(size_t)j * M + i]);
-  int r = i + 1 == M ? 0 : i + 1;
-  if (j < 0) return wall_ghost<true>(__ldg(&Qs[i]), __ldg(&V[i]), __ldg(&V[r]));
+  if (j < 0) {
+    const float4 f = __ldg(&Mj[i]);
+    return wall_ghost_n<true>(__ldg(&Qs[i]), f.x, f.y);
+  }
   if (j <= N + 1) {
+    const float4 f = __ldg(&Mj[(size_t)N * M + i]);
     float4 g1, g2;
-    size_t vb = (size_t)N * M;
-    far_ghosts<true>(__ldg(&Qs[(size_t)(N - 1) * M + i]), __ldg(&V[vb + i]), __ldg(&V[vb + r]), c, g1, g2);
+    far_ghosts_n<true>(__ldg(&Qs[(size_t)(N - 1) * M + i]), f.x, f.y, c, g1, g2);
     return j == N ? g1 : g2;
   }
   return make_float4(1.0f, 0.0f, 0.0f, 1.0f);  // beyond the far field: never read by a valid face
@@ -53,21 +63,53 @@ __device__ __forceinline__ void halo_entry(int tx, int ty, int& hr, int& hc) {
   }
 }
 
-// Flux x length of every face of the tile.  Vs is the vertex tile with row width VW.
-template <int SCHEME, int VW>
-__device__ __forceinline__ void faces_phase(const float4 (*P)[PW], const float2* Vs, float4 (*Fi)[TX + 1],
-                                            float4 (*Fj)[TX], const Consts& c, int i0, int j0, int M, int N, int tx,
-                                            int ty) {
+// Face records of the tile from global memory (per-thread loads; the TMA kernel loads
+// the same boxes with the tensor engine).  Ti[r][cc] = Mi[j0+r][i0+cc] (cc = TX wraps
+// through the seam), Tj[r][cc] = Mj[j0+r][i0+cc]; rows past the grid are left unset.
+__device__ __forceinline__ void stage_faces(const float4* __restrict__ Mi, const float4* __restrict__ Mj,
+                                            float4 (*Ti)[TX + 1], float4 (*Tj)[TX], int i0, int j0, int ic, int M,
+                                            int N, int tx, int ty) {
+#pragma unroll
+  for (int r = ty; r < TY; r += NWY) {
+    const int j = j0 + r;
+    if (j < N) {
+      Ti[r][tx] = __ldg(&Mi[(size_t)j * M + ic]);
+      if (tx == 0) Ti[r][TX] = __ldg(&Mi[(size_t)j * M + wrap_i(i0 + TX, M)]);
+    }
+  }
+  for (int r = ty; r <= TY; r += NWY) {
+    const int j = j0 + r;
+    if (j <= N) Tj[r][tx] = __ldg(&Mj[(size_t)j * M + ic]);
+  }
+}
+
+// 1/A and wave-speed factor of the two owned cells, read before the face phase
+// overwrites the records
+struct FaceW {
+  float iA[2], W[2];
+};
+__device__ __forceinline__ FaceW own_weights(const float4 (*Ti)[TX + 1], const float4 (*Tj)[TX], int tx, int ty) {
+  FaceW w;
+  w.iA[0] = Ti[ty][tx].w;
+  w.iA[1] = Ti[ty + 8][tx].w;
+  w.W[0] = Tj[ty][tx].w;
+  w.W[1] = Tj[ty + 8][tx].w;
+  return w;
+}
+
+// Flux x length of every face of the tile, written over the face's record.
+template <int SCHEME>
+__device__ __forceinline__ void faces_phase(const float4 (*P)[PW], float4 (*Ti)[TX + 1], float4 (*Tj)[TX],
+                                            const Consts& c, int i0, int j0, int M, int N, int tx, int ty) {
   const int nI = ty == 1 && tx < TY ? 3 : 2;
   for (int t = 0; t < nI; t++) {
     const int r = t < 2 ? ty + 8 * t : tx;
     const int cc = t < 2 ? tx : TX;
     if (j0 + r < N && cc <= M - i0) {
-      float nx, ny, len;
-      edge_normal<true>(Vs[(r + 1) * VW + cc], Vs[r * VW + cc], nx, ny, len);  // tangent V(i,j+1)-V(i,j)
+      const float4 m = Ti[r][cc];
       const float4* b = &P[r + 2][cc];
-      float4 f = face_flux<SCHEME, true>(b[0], b[1], b[2], b[3], nx, ny, c);
-      Fi[r][cc] = make_float4(f.x * len, f.y * len, f.z * len, f.w * len);
+      float4 f = face_flux<SCHEME, true>(b[0], b[1], b[2], b[3], m.x, m.y, c);
+      Ti[r][cc] = make_float4(f.x * m.z, f.y * m.z, f.z * m.z, f.w * m.z);
     }
   }
   const int nJ = ty == 0 ? 3 : 2;
@@ -75,22 +117,21 @@ __device__ __forceinline__ void faces_phase(const float4 (*P)[PW], const float2*
     const int r = t < 2 ? ty + 8 * t : TY;
     const int cc = tx;
     if (j0 + r <= N && i0 + cc < M) {
-      float nx, ny, len;
-      edge_normal<true>(Vs[r * VW + cc], Vs[r * VW + cc + 1], nx, ny, len);  // tangent V(i,j)-V(i+1,j)
+      const float4 m = Tj[r][cc];
       const float4* b = &P[r][cc + 2];
-      float4 f = face_flux<SCHEME, true>(b[0], b[PW], b[2 * PW], b[3 * PW], nx, ny, c);
-      Fj[r][cc] = make_float4(f.x * len, f.y * len, f.z * len, f.w * len);
+      float4 f = face_flux<SCHEME, true>(b[0], b[PW], b[2 * PW], b[3 * PW], m.x, m.y, c);
+      Tj[r][cc] = make_float4(f.x * m.z, f.y * m.z, f.z * m.z, f.w * m.z);
     }
   }
 }
 
-// Residual and stage combination of the two owned cells; returns the max wave-speed
-// bits of the new state when EMIT.  qn(h) fetches Qn of owned cell h (stages 2, 3).
-template <int STAGE, bool EMIT, int VW, class QnFetch>
-__device__ __forceinline__ uint32_t combine_phase(const float2* Vs, const float4 (*Fi)[TX + 1],
-                                                  const float4 (*Fj)[TX], float4 qa, float4 qb, QnFetch qn,
-                                                  float4* __restrict__ Qo, float dt, const Consts& c, int i0, int j0,
-                                                  int M, int N, int tx, int ty) {
+// Residual and stage combination of the two owned cells from the face fluxes Fi (over
+// Ti) and Fj (over Tj); returns the max wave-speed bits of the new state when EMIT.
+// qn(h) fetches Qn of owned cell h (stages 2, 3).
+template <int STAGE, bool EMIT, class QnFetch>
+__device__ __forceinline__ uint32_t combine_phase(const float4 (*Fi)[TX + 1], const float4 (*Fj)[TX], const FaceW& w,
+                                                  float4 qa, float4 qb, QnFetch qn, float4* __restrict__ Qo, float dt,
+                                                  const Consts& c, int i0, int j0, int M, int N, int tx, int ty) {
   uint32_t wmax = 0u;
   const int i = i0 + tx;
 #pragma unroll
@@ -99,9 +140,7 @@ __device__ __forceinline__ uint32_t combine_phase(const float2* Vs, const float4
     const int j = j0 + r;
     if (i < M && j < N) {
       const float4 q = h ? qb : qa;
-      float2 a = Vs[r * VW + tx], b = Vs[r * VW + tx + 1], cv = Vs[(r + 1) * VW + tx], d = Vs[(r + 1) * VW + tx + 1];
-      float A = quad_area(a, b, cv, d);
-      float iA = frcp<true>(A);
+      const float iA = w.iA[h];
       float4 fl = Fi[r][tx], fr = Fi[r][tx + 1], fd = Fj[r][tx], fu = Fj[r + 1][tx];
       float4 R;
       R.x = -(((fr.x - fl.x) + fu.x) - fd.x) * iA;
@@ -124,14 +163,7 @@ __device__ __forceinline__ uint32_t combine_phase(const float2* Vs, const float4
                           (n.z + 2.0f * (q.z + dt * R.z)) * third, (n.w + 2.0f * (q.w + dt * R.w)) * third);
       }
       Qo[(size_t)j * M + i] = out;
-      if constexpr (EMIT) {
-        float ll = sqrtf((a.x - cv.x) * (a.x - cv.x) + (a.y - cv.y) * (a.y - cv.y));
-        float lr = sqrtf((b.x - d.x) * (b.x - d.x) + (b.y - d.y) * (b.y - d.y));
-        float lu = sqrtf((cv.x - d.x) * (cv.x - d.x) + (cv.y - d.y) * (cv.y - d.y));
-        float ld = sqrtf((a.x - b.x) * (a.x - b.x) + (a.y - b.y) * (a.y - b.y));
-        float w = wave_speed<true>(out, ((ll + lr) + lu) + ld, A, c.gamma);
-        wmax = max(wmax, __float_as_uint(w));
-      }
+      if constexpr (EMIT) wmax = max(wmax, __float_as_uint(wave_speed_w<true>(out, w.W[h], c.gamma)));
     }
   }
   return wmax;

@@ -16,7 +16,7 @@ def ausm_mod():
 def test_request_bytes(ausm_mod):
     r = ausm_mod.make_request(256, 128)
     M, N = 256, 128
-    assert ausm_mod.request_bytes(r) == 8 * M * (N + 1) + 48 * M * N + 8 * M + 65536
+    assert ausm_mod.request_bytes(r) == 40 * M * (N + 1) + 16 * M * N + 48 * M * N + 8 * M + 65536
 
 
 BAD = [
