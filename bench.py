@@ -490,7 +490,7 @@ def main():
                 "traffic": traffic, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind ==
                 "measured" else "fallback 6650 GB/s",
                 "bytes_per_cell_step": ALG_BYTES_PER_CELL_STEP,
-                "kernel": "k_fused_stage (3 launches per RK3 step; achieved over the whole step)"}
+                "kernel": "k_fused_tile_tma (3 launches per RK3 step; achieved over the whole step)"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
