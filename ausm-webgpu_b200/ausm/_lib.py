@@ -19,7 +19,7 @@ HEADER = ROOT / "include" / "ausm.h"
 OK = 0
 ERR_INVALID, ERR_CUDA, ERR_OOM, ERR_DIVERGED, ERR_STATE, ERR_BUDGET, ERR_TIMEOUT, ERR_NOT_FOUND = range(-1, -9, -1)
 SCHEMES = {"SLAU2": 0, "SLAU": 1, "AUSM+-up": 2}
-ENGINES = {"fused": 0, "reference": 1}
+ENGINES = {"fused": 0, "reference": 1, "f64": 2}
 INIT = {"rest": 0, "freestream": 1}
 OUTER = {"rect": 0, "circle": 1}
 GRID = {"jacobi": 0, "multicolor": 1}
@@ -90,6 +90,7 @@ _SIGS = {
     "ausm_init_state": [_P, C.c_int],
     "ausm_set_state": [_P, C.POINTER(C.c_float)],
     "ausm_get_state": [_P, C.POINTER(C.c_float)],
+    "ausm_get_state_f64": [_P, C.POINTER(C.c_double)],
     "ausm_step": [_P, C.c_int, C.POINTER(C.c_float)],
     "ausm_max_wave_speed": [_P, C.POINTER(C.c_float)],
     "ausm_forces": [_P, C.POINTER(C.c_double), C.POINTER(C.c_double)],

@@ -160,6 +160,12 @@ class Solver:
         self._c(lib().ausm_get_state(self.h, _fp(a)))
         return a
 
+    def state_f64(self) -> np.ndarray:
+        """State in the reference layout in double (the F64 engine's own; FP32 engines' widened)."""
+        a = np.zeros((self.N + 3, self.M, 4), dtype=np.float64)
+        self._c(lib().ausm_get_state_f64(self.h, _dp(a)))
+        return a
+
     def step(self, n: int = 1, wait: bool = True) -> float | None:
         """n RK3 steps with dt fixed from the current state; returns that dt (f32)."""
         if not wait:

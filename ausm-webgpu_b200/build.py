@@ -26,7 +26,7 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-I", str(ROOT / "include"), "-I", str(CSRC),
           "-Xptxas", "-v", "--expt-relaxed-constexpr"]
-NO_FMAD = {"kernels_reference.cu", "kernels_misc.cu"}
+NO_FMAD = {"kernels_reference.cu", "kernels_misc.cu", "kernels_f64.cu"}
 EXTRA = os.environ.get("AUSM_NVCC_EXTRA", "").split()  # tuning sweeps, e.g. -DAUSM_FUSED_MIN_BLOCKS=4
 
 

@@ -43,6 +43,23 @@ void make_consts(ausm_solver* h) {
   c.gmgm1 = g / c.gm1;
   c.muscl = p.muscl;
   h->c = c;
+  // FP64 constants from the FP64 parameters, in the oracle's operation order
+  ex::ConstsR<double> d{};
+  d.gamma = p.gamma; d.inRho = p.in_rho; d.inP = p.in_pressure;
+  d.gm1 = p.gamma - 1.0;
+  d.gm1inv = 1.0 / (p.gamma - 1.0);
+  d.Kp = p.K_p; d.Ku = p.K_u; d.cfl = p.cfl; d.maxdt = p.maxdt;
+  d.inflow = {u, v};
+  d.inState = {p.in_rho, u * p.in_rho, v * p.in_rho, rhoE};
+  d.a2inf = (p.gamma * p.in_pressure) / p.in_rho;
+  d.Vinf2 = u * u + v * v;
+  d.Minf2 = d.Vinf2 / d.a2inf;
+  d.gammaInP = p.gamma * p.in_pressure;
+  d.aStarK = (2.0 * d.gm1) / (p.gamma + 1.0);
+  d.ambE = p.in_pressure / (p.gamma - 1.0);
+  d.muscl = p.muscl;
+  h->cd = d;
+  if (h->f64) h->f64->c = d;
 }
 
 void ramp_after_steps(ausm_solver* h, int n) {
@@ -98,8 +115,10 @@ int ensure_reference_buffers(ausm_solver* h) {
   CU(h, dalloc(&h->area, n));
   return AUSM_OK;
 }
+// staging: a float reference-layout state (M x (N+3) float4) followed by room for one
+// M x N float field
 int ensure_staging(ausm_solver* h) {
-  if (!h->staging) CU(h, dalloc(&h->staging, (size_t)h->M * (h->N + 3)));
+  if (!h->staging) CU(h, dalloc(&h->staging, (size_t)h->M * (h->N + 3) + ((size_t)h->M * h->N + 3) / 4));
   return AUSM_OK;
 }
 
@@ -108,7 +127,55 @@ const float4* interior(ausm_solver* h) {
   return h->engine == AUSM_ENGINE_FUSED ? h->Q[h->cur] : h->S[2] + h->M;
 }
 
+// The current state in the float reference layout, in staging.
+int state_to_staging(ausm_solver* h) {
+  int rc = ensure_staging(h);
+  if (rc) return rc;
+  if (h->engine == AUSM_ENGINE_FUSED)
+    launch_to_ref_layout(h->Q[h->cur], h->staging, h->V, h->c, h->M, h->N, h->st);
+  else if (h->engine == AUSM_ENGINE_REFERENCE)
+    launch_ref_boundary(h->S[2], h->staging, h->V, h->c, h->M, h->N, h->st);
+  else
+    h->f64->to_f32(h->staging, h->Vd, h->st);
+  CHECK_LAUNCH(h);
+  return AUSM_OK;
+}
+// A float reference-layout state in staging becomes the current engine's state.
+int staging_to_state(ausm_solver* h) {
+  if (h->engine == AUSM_ENGINE_FUSED) {
+    h->cur = 0;
+    launch_from_ref_layout(h->staging, h->Q[0], h->M, h->N, h->st);
+  } else if (h->engine == AUSM_ENGINE_REFERENCE) {
+    CU(h, cudaMemcpyAsync(h->S[2], h->staging, (size_t)h->M * (h->N + 3) * sizeof(float4), cudaMemcpyDeviceToDevice,
+                          h->st));
+  } else {
+    h->f64->from_f32(h->staging, h->st);
+  }
+  CHECK_LAUNCH(h);
+  return AUSM_OK;
+}
+int ensure_f64(ausm_solver* h) {
+  if (h->f64) return AUSM_OK;
+  h->f64 = new F64Engine();
+  cudaError_t e = h->f64->allocate(h->M, h->N);
+  if (e != cudaSuccess) {
+    delete h->f64;
+    h->f64 = nullptr;
+    return fail(h, e == cudaErrorMemoryAllocation ? AUSM_ERR_OOM : AUSM_ERR_CUDA,
+                std::string("FP64 engine buffers: ") + cudaGetErrorString(e));
+  }
+  h->f64->c = h->cd;
+  if (h->has_grid) h->f64->metrics(h->Vd, h->st);
+  CHECK_LAUNCH(h);
+  return AUSM_OK;
+}
+
 int refresh_wave(ausm_solver* h) {
+  if (h->engine == AUSM_ENGINE_F64) {
+    h->f64->wave_speed(h->st);
+    CHECK_LAUNCH(h);
+    return AUSM_OK;
+  }
   CU(h, cudaMemsetAsync(h->wave, 0, sizeof(uint32_t), h->st));
   if (h->engine == AUSM_ENGINE_FUSED) {
     launch_wave_interior(h->Q[h->cur], h->Mj, h->c.gamma, h->M, h->N, h->wave, h->st);
@@ -121,6 +188,7 @@ int refresh_wave(ausm_solver* h) {
 
 int after_grid(ausm_solver* h) {
   launch_metrics_d(h->Vd, h->Mi, h->Mj, h->M, h->N, h->st);
+  if (h->f64) h->f64->metrics(h->Vd, h->st);
   CHECK_LAUNCH(h);
   if (h->engine == AUSM_ENGINE_REFERENCE) {
     launch_ref_metrics(h->V, h->area, h->flen, h->M, h->N, h->st);
@@ -213,6 +281,7 @@ int ausm_destroy(ausm_solver* h) {
                    h->flen, h->area, h->staging, h->cp, h->wave, h->dt, h->dacc, h->parts, h->move, h->err_flag};
   for (void* d : dptrs)
     if (d) cudaFree(d);
+  delete h->f64;
   if (h->h_dt) cudaFreeHost(h->h_dt);
   if (h->h_wave) cudaFreeHost(h->h_wave);
   if (h->h_acc) cudaFreeHost(h->h_acc);
@@ -297,7 +366,8 @@ int ausm_dims(const ausm_solver* h, int* M, int* N) {
 
 int ausm_set_engine(ausm_solver* h, int engine) {
   NEED(h, h, AUSM_ERR_INVALID, "null handle");
-  NEED(h, engine == AUSM_ENGINE_FUSED || engine == AUSM_ENGINE_REFERENCE, AUSM_ERR_INVALID, "unknown engine");
+  NEED(h, engine == AUSM_ENGINE_FUSED || engine == AUSM_ENGINE_REFERENCE || engine == AUSM_ENGINE_F64,
+       AUSM_ERR_INVALID, "unknown engine");
   if (engine == h->engine) return AUSM_OK;
   NEED(h, !h->batch, AUSM_ERR_STATE, "a batch member stays on the fused engine; remove it from the batch first");
   int rc = use_device(h);
@@ -309,14 +379,13 @@ int ausm_set_engine(ausm_solver* h, int engine) {
       launch_ref_metrics(h->V, h->area, h->flen, h->M, h->N, h->st);
       CHECK_LAUNCH(h);
     }
-    if (h->has_state) {
-      launch_to_ref_layout(h->Q[h->cur], h->S[2], h->V, h->c, h->M, h->N, h->st);
-      CHECK_LAUNCH(h);
-    }
-  } else if (h->has_state) {
-    h->cur = 0;
-    launch_from_ref_layout(h->S[2], h->Q[0], h->M, h->N, h->st);
-    CHECK_LAUNCH(h);
+  }
+  if (engine == AUSM_ENGINE_F64 && (rc = ensure_f64(h))) return rc;
+  if (h->has_state) {  // carry the state over through the float reference layout
+    if ((rc = state_to_staging(h))) return rc;
+    h->engine = engine;
+    if ((rc = staging_to_state(h))) return rc;
+    return refresh_wave(h);
   }
   h->engine = engine;
   return AUSM_OK;
@@ -543,8 +612,12 @@ int ausm_init_state(ausm_solver* h, int mode) {
   if (h->engine == AUSM_ENGINE_FUSED) {
     h->cur = 0;
     launch_fill(h->Q[0], s, (size_t)h->M * h->N, h->st);
-  } else {
+  } else if (h->engine == AUSM_ENGINE_REFERENCE) {
     launch_fill(h->S[2], s, (size_t)h->M * (h->N + 3), h->st);
+  } else {
+    const ex::ConstsR<double>& d = h->cd;
+    if (mode == AUSM_INIT_REST) h->f64->fill(d.inRho, 0.0, 0.0, d.inP / (d.gamma - 1.0), h->st);
+    else h->f64->fill(d.inState.x, d.inState.y, d.inState.z, d.inState.w, h->st);
   }
   CHECK_LAUNCH(h);
   h->has_state = true;
@@ -558,15 +631,12 @@ int ausm_set_state(ausm_solver* h, const float* q) {
   int rc = use_device(h);
   if (rc) return rc;
   size_t bytes = (size_t)h->M * (h->N + 3) * sizeof(float4);
-  if (h->engine == AUSM_ENGINE_FUSED) {
-    rc = ensure_staging(h);
-    if (rc) return rc;
-    CU(h, cudaMemcpyAsync(h->staging, q, bytes, cudaMemcpyHostToDevice, h->st));
-    h->cur = 0;
-    launch_from_ref_layout(h->staging, h->Q[0], h->M, h->N, h->st);
-    CHECK_LAUNCH(h);
-  } else {
+  if (h->engine == AUSM_ENGINE_REFERENCE) {
     CU(h, cudaMemcpyAsync(h->S[2], q, bytes, cudaMemcpyHostToDevice, h->st));
+  } else {
+    if ((rc = ensure_staging(h))) return rc;
+    CU(h, cudaMemcpyAsync(h->staging, q, bytes, cudaMemcpyHostToDevice, h->st));
+    if ((rc = staging_to_state(h))) return rc;
   }
   h->has_state = true;
   return refresh_wave(h);
@@ -578,15 +648,29 @@ int ausm_get_state(ausm_solver* h, float* q) {
   NEED(h, h->has_state, AUSM_ERR_STATE, "no state yet");
   int rc = use_device(h);
   if (rc) return rc;
-  rc = ensure_staging(h);
-  if (rc) return rc;
-  if (h->engine == AUSM_ENGINE_FUSED)
-    launch_to_ref_layout(h->Q[h->cur], h->staging, h->V, h->c, h->M, h->N, h->st);
-  else
-    launch_ref_boundary(h->S[2], h->staging, h->V, h->c, h->M, h->N, h->st);
-  CHECK_LAUNCH(h);
+  if ((rc = state_to_staging(h))) return rc;
   CU(h, cudaMemcpyAsync(q, h->staging, (size_t)h->M * (h->N + 3) * sizeof(float4), cudaMemcpyDeviceToHost, h->st));
   CU(h, cudaStreamSynchronize(h->st));
+  return AUSM_OK;
+}
+
+int ausm_get_state_f64(ausm_solver* h, double* q) {
+  NEED(h, h, AUSM_ERR_INVALID, "null handle");
+  NEED(h, q, AUSM_ERR_INVALID, "null state");
+  NEED(h, h->has_state, AUSM_ERR_STATE, "no state yet");
+  int rc = use_device(h);
+  if (rc) return rc;
+  const size_t n = (size_t)h->M * (h->N + 3);
+  if (h->engine == AUSM_ENGINE_F64) {
+    const void* src = h->f64->state_ref(h->Vd, h->st);
+    CHECK_LAUNCH(h);
+    CU(h, cudaMemcpyAsync(q, src, n * 4 * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+    CU(h, cudaStreamSynchronize(h->st));
+    return AUSM_OK;
+  }
+  std::vector<float> f(n * 4);
+  if ((rc = ausm_get_state(h, f.data()))) return rc;
+  for (size_t k = 0; k < f.size(); k++) q[k] = f[k];
   return AUSM_OK;
 }
 
@@ -598,6 +682,20 @@ int ausm_step(ausm_solver* h, int n, float* dt_out) {
   if (rc) return rc;
   const int M = h->M, N = h->N, sch = h->p.scheme;
   cudaStream_t s = h->st;
+  if (h->engine == AUSM_ENGINE_F64) {
+    h->f64->step(sch, n, h->Vd, s);
+    CHECK_LAUNCH(h);
+    ramp_after_steps(h, n);
+    if (dt_out) {
+      CU(h, cudaMemcpyAsync(h->h_acc, h->f64->dt, sizeof(double), cudaMemcpyDeviceToHost, s));
+      CU(h, cudaMemcpyAsync(h->h_acc + 1, h->f64->wave, sizeof(double), cudaMemcpyDeviceToHost, s));
+      CU(h, cudaStreamSynchronize(s));
+      *dt_out = (float)h->h_acc[0];
+      if (!std::isfinite(h->h_acc[1]) || !std::isfinite(h->h_acc[0]))
+        return fail(h, AUSM_ERR_DIVERGED, "max wave speed is not finite: the solution diverged");
+    }
+    return AUSM_OK;
+  }
   launch_dt(h->wave, h->dt, h->c.maxdt, h->c.cfl, s);
   if (n > 0) {
     CU(h, cudaMemsetAsync(h->wave, 0, sizeof(uint32_t), s));
@@ -665,6 +763,12 @@ int ausm_max_wave_speed(ausm_solver* h, float* out) {
   NEED(h, out, AUSM_ERR_INVALID, "null output");
   int rc = use_device(h);
   if (rc) return rc;
+  if (h->engine == AUSM_ENGINE_F64) {
+    CU(h, cudaMemcpyAsync(h->h_acc, h->f64->wave, sizeof(double), cudaMemcpyDeviceToHost, h->st));
+    CU(h, cudaStreamSynchronize(h->st));
+    *out = (float)h->h_acc[0];
+    return AUSM_OK;
+  }
   CU(h, cudaMemcpyAsync(h->h_wave, h->wave, sizeof(uint32_t), cudaMemcpyDeviceToHost, h->st));
   CU(h, cudaStreamSynchronize(h->st));
   std::memcpy(out, h->h_wave, 4);
@@ -681,8 +785,11 @@ int ausm_forces(ausm_solver* h, double* out6, double* cp) {
   double vx = h->speed_now * std::cos(a), vy = h->speed_now * std::sin(a);
   double q_inf = 0.5 * p.in_rho * (vx * vx + vy * vy);
   if (cp && !h->cp) CU(h, dalloc(&h->cp, (size_t)h->M));
-  launch_forces(interior(h), h->Vd, h->c, h->M, h->dacc, h->parts, cp ? h->cp : nullptr, q_inf, p.in_pressure,
-                h->st);
+  if (h->engine == AUSM_ENGINE_F64)
+    h->f64->forces(h->Vd, h->parts, h->dacc, cp ? h->cp : nullptr, q_inf, p.in_pressure, h->st);
+  else
+    launch_forces(interior(h), h->Vd, h->c, h->M, h->dacc, h->parts, cp ? h->cp : nullptr, q_inf, p.in_pressure,
+                  h->st);
   CHECK_LAUNCH(h);
   CU(h, cudaMemcpyAsync(h->h_acc, h->dacc, 2 * sizeof(double), cudaMemcpyDeviceToHost, h->st));
   if (cp) CU(h, cudaMemcpyAsync(cp, h->cp, (size_t)h->M * sizeof(double), cudaMemcpyDeviceToHost, h->st));
@@ -711,8 +818,11 @@ int ausm_residual_l2(ausm_solver* h, double* l2) {
   int rc = use_device(h);
   if (rc) return rc;
   const int M = h->M, N = h->N;
-  const float4* R;
-  if (h->engine == AUSM_ENGINE_FUSED) {
+  const float4* R = nullptr;
+  if (h->engine == AUSM_ENGINE_F64) {
+    h->f64->residual(h->p.scheme, h->Vd, h->st);
+    h->f64->sumsq_rho(h->parts, h->dacc, h->st);
+  } else if (h->engine == AUSM_ENGINE_FUSED) {
     float4* scratch = h->Q[(h->cur + 1) % 3];
     launch_fused_stage(h->p.scheme, 0, false, h->Q[h->cur], nullptr, scratch, h->Mi, h->Mj, h->dt, h->wave, h->c, M, N,
                        nullptr, h->err_flag, h->st);
@@ -723,7 +833,7 @@ int ausm_residual_l2(ausm_solver* h, double* l2) {
     launch_ref_residual(h->fx, h->fy, h->flen, h->area, h->res, M, N, h->st);
     R = h->res;
   }
-  launch_sumsq_rho(R, (size_t)M * N, h->dacc, h->parts, h->st);
+  if (R) launch_sumsq_rho(R, (size_t)M * N, h->dacc, h->parts, h->st);
   CHECK_LAUNCH(h);
   CU(h, cudaMemcpyAsync(h->h_acc, h->dacc, sizeof(double), cudaMemcpyDeviceToHost, h->st));
   CU(h, cudaStreamSynchronize(h->st));
@@ -741,8 +851,16 @@ int ausm_field(ausm_solver* h, int kind, float* out) {
   if (rc) return rc;
   rc = ensure_staging(h);
   if (rc) return rc;
+  const float4* q;
   float* buf = reinterpret_cast<float*>(h->staging);
-  launch_field(interior(h), h->V, h->c, kind, h->M, h->N, buf, h->st);
+  if (h->engine == AUSM_ENGINE_F64) {  // rounded to f32 into staging; the field goes past it
+    if ((rc = state_to_staging(h))) return rc;
+    q = h->staging + h->M;
+    buf = reinterpret_cast<float*>(h->staging + (size_t)h->M * (h->N + 3));
+  } else {
+    q = interior(h);
+  }
+  launch_field(q, h->V, h->c, kind, h->M, h->N, buf, h->st);
   CHECK_LAUNCH(h);
   CU(h, cudaMemcpyAsync(out, buf, (size_t)h->M * h->N * sizeof(float), cudaMemcpyDeviceToHost, h->st));
   CU(h, cudaStreamSynchronize(h->st));

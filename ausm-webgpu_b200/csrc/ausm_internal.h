@@ -7,6 +7,7 @@
 #include <algorithm>
 
 #include "physics.cuh"
+#include "physics_exact.cuh"
 
 namespace ausm {
 
@@ -104,6 +105,33 @@ void launch_batch_gather(const BatchSolve* d, int nsolves, float* out, cudaStrea
 // part holds one double per tile.  Summation order depends only on the solve's own grid.
 void launch_batch_residual_norm(const BatchSolve* d, int nsolves, int total_tiles, double* part, double* l2,
                                 cudaStream_t s);
+
+// ---- full-FP64 engine (kernels_f64.cu, built with -fmad=false) ----
+// The reference-shaped engine in double on its own buffers; vertices are the solver's
+// FP64 vertices.  S[2] holds the current state in the reference layout.
+struct F64Engine {
+  int M = 0, N = 0;
+  ex::ConstsR<double> c{};
+  ex::V4<double>* S[3] = {nullptr, nullptr, nullptr};
+  ex::V4<double>*fx = nullptr, *fy = nullptr, *res = nullptr, *flen = nullptr;
+  double* area = nullptr;
+  unsigned long long* wave = nullptr;  // max wave speed, double bits
+  double* dt = nullptr;
+  ~F64Engine();
+  cudaError_t allocate(int M, int N);
+  void metrics(const double2* Vd, cudaStream_t s);
+  void from_f32(const float4* ref, cudaStream_t s);  // a float reference-layout state -> S[2]
+  void to_f32(float4* ref, const double2* Vd, cudaStream_t s);
+  void fill(double rho, double ru, double rv, double E, cudaStream_t s);
+  const void* state_ref(const double2* Vd, cudaStream_t s);  // S[2] with its ghost rows, in S[0]
+  void wave_speed(cudaStream_t s);
+  void step(int scheme, int n, const double2* Vd, cudaStream_t s);
+  void residual(int scheme, const double2* Vd, cudaStream_t s);  // dQ/dt of S[2] into res
+  void sumsq_rho(double* parts, double* acc, cudaStream_t s);
+  void forces(const double2* Vd, double* parts, double* acc, double* cp, double q_inf, double p_inf, cudaStream_t s);
+};
+// out[q] = fixed-order sum of parts[q * kMaxParts + 0 .. nb - 1], q < nq (kernels_misc.cu)
+void launch_sum_parts(const double* parts, int nb, int nq, double* out, cudaStream_t s);
 
 // ---- reference-shaped engine (kernels_reference.cu, built with -fmad=false) ----
 // States use the reference layout [N+3][M] (row 0 wall ghost).

@@ -317,6 +317,9 @@ void launch_f2d(const float2* a, double2* b, size_t n, cudaStream_t s) { k_f2d<<
 void launch_metrics_d(const double2* V, float4* Mi, float4* Mj, int M, int N, cudaStream_t s) {
   k_metrics_d<<<grid16(M, N + 1), B16, 0, s>>>(V, Mi, Mj, M, N);
 }
+void launch_sum_parts(const double* parts, int nb, int nq, double* out, cudaStream_t s) {
+  k_sum_parts<<<nq, 256, 0, s>>>(parts, nb, out);
+}
 void launch_field(const float4* Qint, const float2* V, const Consts& c, int kind, int M, int N, float* out,
                   cudaStream_t s) {
   k_field<<<grid16(M, N), B16, 0, s>>>(Qint, V, c, kind, M, N, out);

@@ -12,6 +12,8 @@ struct ausm_solver {
   AusmParams p{};
   double speed_now = 0.0;  // current inflow speed (ramped when p.ramp > 0)
   ausm::Consts c{};
+  ausm::ex::ConstsR<double> cd{};  // the same constants in FP64 (F64 engine)
+  ausm::F64Engine* f64 = nullptr;  // buffers of the F64 engine, once selected
   cudaStream_t st = nullptr;      // the stream calls run on (the batch's while a member)
   cudaStream_t own_st = nullptr;  // the handle's own stream
   ausm_batch* batch = nullptr;    // batch this solver belongs to, if any

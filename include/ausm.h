@@ -62,6 +62,7 @@ extern "C" {
  * dispatches per stage (boundary, j-flux, i-flux, residual, RK combine) */
 #define AUSM_ENGINE_FUSED 0
 #define AUSM_ENGINE_REFERENCE 1
+#define AUSM_ENGINE_F64 2 /* the reference-shaped engine in FP64 (precision study) */
 
 /* headless field outputs (ausm.js:617-707 without colour mapping) */
 #define AUSM_FIELD_DENSITY 0
@@ -145,6 +146,9 @@ int ausm_init_state(ausm_solver* h, int mode);
  * of the boundary pass applied to that interior (ausm.js:34-120). */
 int ausm_set_state(ausm_solver* h, const float* q);
 int ausm_get_state(ausm_solver* h, float* q);
+/* The same layout in double: the F64 engine's state as it is, the FP32 engines' state
+ * widened (no counterpart in the reference, which is FP32 only). */
+int ausm_get_state_f64(ausm_solver* h, double* q);
 
 /* step(n): dt = min(maxdt, cfl / max wave speed) of the current state, held for n
  * TVD-RK3 steps, then the max wave speed of the new state (main.js:744-791).  dt_out
