@@ -202,6 +202,13 @@ class Solver:
     def synchronize(self):
         self._c(lib().ausm_synchronize(self.h))
 
+    def autotune(self, force: bool = False) -> int:
+        """Tile height (8, 16 or 32 rows) of the fused stage kernel for this solve, measured
+        on first use (or again with force); returns the height in use."""
+        r = C.c_int()
+        self._c(lib().ausm_autotune(self.h, int(bool(force)), C.byref(r)))
+        return r.value
+
     def time_steps(self, n: int, reps: int) -> float:
         """Device time (ms) of `reps` calls of step(n), CUDA events on the solver's stream."""
         ms = C.c_float()

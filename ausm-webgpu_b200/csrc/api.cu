@@ -4,7 +4,10 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include "ausm.h"
@@ -68,6 +71,82 @@ void ramp_after_steps(ausm_solver* h, int n) {
     h->speed_now += (target - h->speed_now) / (h->p.ramp / n * 50.0);
     make_consts(h);
   }
+}
+
+// ---- tile-height autotuner ----
+// The TMA stage kernel exists for tile heights 8, 16 and 32 (32 x 4, 32 x 8 and 32 x 16
+// threads; 8, 4 and 2 CTAs per SM).  Which is fastest depends on the grid (partial
+// tiles at the edges, halo overhead, occupancy) and the scheme, so it is measured: a
+// few stage-1 launches per candidate on the solve's own data, timed with CUDA events on
+// its stream.  Stage 1 reads the current state and writes the next buffer, which is
+// scratch until the next step's stage 1 overwrites it, so tuning has no effect on the
+// solution.  Results are cached per (M, N, scheme) for the process.
+namespace {
+std::mutex g_tune_mu;
+std::map<std::tuple<int, int, int>, int> g_tune_cache;
+}  // namespace
+
+int tuned_tile_rows(ausm_solver* h, bool force, int* rows) {
+  *rows = 16;
+  if (!h->tma[1].ok) return AUSM_OK;  // per-thread kernels: 16 rows
+  if (const char* e = std::getenv("AUSM_TILE_ROWS")) {
+    const int r = std::atoi(e);
+    if ((r == 8 || r == 16 || r == 32) && h->tma[tile_index(r)].ok) {
+      *rows = r;
+      return AUSM_OK;
+    }
+  }
+  if (const char* e = std::getenv("AUSM_AUTOTUNE"))
+    if (e[0] == '0') return AUSM_OK;
+  if (!force && h->tile_rows) {
+    *rows = h->tile_rows;
+    return AUSM_OK;
+  }
+  const auto key = std::make_tuple(h->M, h->N, h->p.scheme);
+  if (!force) {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune_cache.find(key);
+    if (it != g_tune_cache.end()) {
+      *rows = h->tile_rows = it->second;
+      return AUSM_OK;
+    }
+  }
+  const int a = h->cur, b = (a + 1) % 3;
+  const double cells = (double)h->M * h->N;
+  const int reps = (int)std::max(3.0, std::min(50.0, 4.0e6 / cells));
+  float best = INFINITY;
+  int best_rows = 16;
+  for (int k = 0; k < 3; k++) {
+    const TmaMaps& tm = h->tma[k];
+    if (!tm.ok) continue;
+    const TmaMapsLaunch t = {tm.halo[a], tm.plain[a], tm.mi, tm.mj};
+    auto launch = [&] {
+      launch_fused_stage(h->p.scheme, 1, false, h->Q[a], nullptr, h->Q[b], h->Mi, h->Mj, h->dt, h->wave, h->c, h->M,
+                         h->N, &t, kTileHeights[k], h->err_flag, h->st);
+    };
+    launch();  // warm-up (first-launch attribute set-up, caches)
+    launch();
+    cudaEventRecord(h->e0, h->st);
+    for (int r = 0; r < reps; r++) launch();
+    cudaEventRecord(h->e1, h->st);
+    cudaError_t e = cudaEventSynchronize(h->e1);
+    if (e == cudaSuccess) e = cudaGetLastError();
+    if (e != cudaSuccess) {
+      set_thread_error(std::string("tile autotuning: ") + cudaGetErrorString(e));
+      h->err = std::string("tile autotuning: ") + cudaGetErrorString(e);
+      return AUSM_ERR_CUDA;
+    }
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, h->e0, h->e1);
+    if (ms < best) {
+      best = ms;
+      best_rows = kTileHeights[k];
+    }
+  }
+  *rows = h->tile_rows = best_rows;
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tune_cache[key] = best_rows;
+  return AUSM_OK;
 }
 
 }  // namespace ausm
@@ -345,7 +424,8 @@ int ausm_create(int M, int N, ausm_solver** out) {
     const float4* qs[3] = {h->Q[0], h->Q[1], h->Q[2]};
     // odd M keeps the per-thread staging kernel; AUSM_NO_TMA=1 selects it for A/B timing
     const char* no_tma = std::getenv("AUSM_NO_TMA");
-    if (!(no_tma && no_tma[0] == '1')) encode_tma_maps(qs, h->Mi, h->Mj, M, N, &h->tma);
+    if (!(no_tma && no_tma[0] == '1'))
+      for (int k = 0; k < 3; k++) encode_tma_maps(qs, h->Mi, h->Mj, M, N, kTileHeights[k], &h->tma[k]);
   }
   ausm_default_params(&h->p);
   h->speed_now = inflow_target(h->p);
@@ -404,6 +484,7 @@ int ausm_set_params(ausm_solver* h, const AusmParams* p) {
   int rc = use_device(h);
   if (rc) return rc;
   bool gamma_changed = p->gamma != h->p.gamma;
+  if (p->scheme != h->p.scheme) h->tile_rows = 0;  // tuned per scheme
   h->p = *p;
   if (p->ramp <= 0.0) h->speed_now = inflow_target(*p);
   make_consts(h);
@@ -420,6 +501,7 @@ int ausm_get_params(const ausm_solver* h, AusmParams* p) {
 int ausm_set_scheme(ausm_solver* h, int scheme) {
   NEED(h, h, AUSM_ERR_INVALID, "null handle");
   NEED(h, scheme >= 0 && scheme <= 2, AUSM_ERR_INVALID, "unknown scheme");
+  if (scheme != h->p.scheme) h->tile_rows = 0;  // tuned per scheme
   h->p.scheme = scheme;
   return AUSM_OK;
 }
@@ -700,22 +782,25 @@ int ausm_step(ausm_solver* h, int n, float* dt_out) {
   if (n > 0) {
     CU(h, cudaMemsetAsync(h->wave, 0, sizeof(uint32_t), s));
     if (h->engine == AUSM_ENGINE_FUSED) {
+      int rows = 16;
+      if ((rc = tuned_tile_rows(h, false, &rows))) return rc;
       for (int k = 0; k < n; k++) {
         int a = h->cur, b = (a + 1) % 3, c3 = (a + 2) % 3;
         TmaMapsLaunch t1, t2, t3;
         const TmaMapsLaunch *p1 = nullptr, *p2 = nullptr, *p3 = nullptr;
-        if (h->tma.ok) {
-          t1 = {h->tma.halo[a], h->tma.plain[a], h->tma.mi, h->tma.mj};
-          t2 = {h->tma.halo[b], h->tma.plain[a], h->tma.mi, h->tma.mj};
-          t3 = {h->tma.halo[c3], h->tma.plain[a], h->tma.mi, h->tma.mj};
+        const TmaMaps& tm = h->tma[tile_index(rows)];
+        if (tm.ok) {
+          t1 = {tm.halo[a], tm.plain[a], tm.mi, tm.mj};
+          t2 = {tm.halo[b], tm.plain[a], tm.mi, tm.mj};
+          t3 = {tm.halo[c3], tm.plain[a], tm.mi, tm.mj};
           p1 = &t1; p2 = &t2; p3 = &t3;
         }
         launch_fused_stage(sch, 1, false, h->Q[a], nullptr, h->Q[b], h->Mi, h->Mj, h->dt, h->wave, h->c, M, N, p1,
-                           h->err_flag, s);
+                           rows, h->err_flag, s);
         launch_fused_stage(sch, 2, false, h->Q[b], h->Q[a], h->Q[c3], h->Mi, h->Mj, h->dt, h->wave, h->c, M, N, p2,
-                           h->err_flag, s);
-        launch_fused_stage(sch, 3, k == n - 1, h->Q[c3], h->Q[a], h->Q[b], h->Mi, h->Mj, h->dt, h->wave, h->c, M, N, p3,
-                           h->err_flag, s);
+                           rows, h->err_flag, s);
+        launch_fused_stage(sch, 3, k == n - 1, h->Q[c3], h->Q[a], h->Q[b], h->Mi, h->Mj, h->dt, h->wave, h->c, M, N,
+                           p3, rows, h->err_flag, s);
         h->cur = b;
       }
     } else {
@@ -825,7 +910,7 @@ int ausm_residual_l2(ausm_solver* h, double* l2) {
   } else if (h->engine == AUSM_ENGINE_FUSED) {
     float4* scratch = h->Q[(h->cur + 1) % 3];
     launch_fused_stage(h->p.scheme, 0, false, h->Q[h->cur], nullptr, scratch, h->Mi, h->Mj, h->dt, h->wave, h->c, M, N,
-                       nullptr, h->err_flag, h->st);
+                       nullptr, 16, h->err_flag, h->st);
     R = scratch;
   } else {
     launch_ref_boundary(h->S[2], h->S[0], h->V, h->c, M, N, h->st);
@@ -877,6 +962,20 @@ int ausm_stream(ausm_solver* h, void** stream) {
 int ausm_synchronize(ausm_solver* h) {
   NEED(h, h, AUSM_ERR_INVALID, "null handle");
   CU(h, cudaStreamSynchronize(h->st));
+  return AUSM_OK;
+}
+
+int ausm_autotune(ausm_solver* h, int force, int* rows) {
+  NEED(h, h, AUSM_ERR_INVALID, "null handle");
+  NEED(h, h->has_grid && h->has_state, AUSM_ERR_STATE, "need a grid and a state");
+  int rc = use_device(h);
+  if (rc) return rc;
+  int r = 16;
+  if (h->engine == AUSM_ENGINE_FUSED) {
+    launch_dt(h->wave, h->dt, h->c.maxdt, h->c.cfl, h->st);
+    if ((rc = tuned_tile_rows(h, force != 0, &r))) return rc;
+  }
+  if (rows) *rows = r;
   return AUSM_OK;
 }
 

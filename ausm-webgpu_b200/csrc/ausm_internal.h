@@ -65,14 +65,19 @@ struct TmaMapsLaunch {  // the four a stage launch reads
   CUtensorMap qn;
   CUtensorMap mi, mj;
 };
-bool encode_tma_maps(const float4* const Q[3], const float4* Mi, const float4* Mj, int M, int N, TmaMaps* out);
+// Tile heights of the TMA tile kernels (the autotuner's candidates) and their index.
+constexpr int kTileHeights[3] = {8, 16, 32};
+bool encode_tma_maps(const float4* const Q[3], const float4* Mi, const float4* Mj, int M, int N, int ty,
+                     TmaMaps* out);
 // stage 1..3: RK stage; stage 0: write dQ/dt of Qs to Qo.  emit (stage 3 only):
 // atomicMax the new state's wave speed bits into *wave (zeroed by the caller).  With
 // tm != nullptr the persistent TMA kernel runs and sets *err on a bounded-wait timeout.
 // Mi, Mj: the FP64-computed face records (launch_metrics_d).
+// ty: tile height of the TMA tile kernel (8, 16 or 32; tm must come from maps of that
+// height); the per-thread and persistent kernels use 16.
 void launch_fused_stage(int scheme, int stage, bool emit, const float4* Qs, const float4* Qn, float4* Qo,
                         const float4* Mi, const float4* Mj, const float* dt, uint32_t* wave, const Consts& c, int M,
-                        int N, const TmaMapsLaunch* tm, int* err, cudaStream_t s);
+                        int N, const TmaMapsLaunch* tm, int ty, int* err, cudaStream_t s);
 void launch_wave_interior(const float4* Q, const float4* Mj, float gamma, int M, int N, uint32_t* wave,
                           cudaStream_t s);
 
@@ -94,17 +99,18 @@ struct BatchSolve {
 // Stage 0 writes the residual dQ/dt of the current state into the solve's next buffer.
 // A stage launch covers one scheme group: descriptors [s_lo, s_hi), items [t_lo, t_hi).
 void launch_batch_dt(BatchSolve* d, int nsolves, cudaStream_t s);
-// With err != nullptr (every solve of the launch has maps) stages 1-3 stage their tiles
-// by TMA and a bounded-wait timeout sets *err.
+// rows: tile height (8, 16, 32) the descriptors' work items were laid out with.  With
+// err != nullptr (every solve of the launch has maps for that height) stages 1-3 stage
+// their tiles by TMA and a bounded-wait timeout sets *err; without TMA rows must be 16.
 void launch_batch_stage(int scheme, int stage, bool emit, const BatchSolve* d, int s_lo, int s_hi, int t_lo,
-                        int t_hi, int rot, int* err, cudaStream_t s);
+                        int t_hi, int rot, int rows, int* err, cudaStream_t s);
 void launch_batch_advance(BatchSolve* d, int nsolves, int steps, cudaStream_t s);
 // out[2 s] = dt, out[2 s + 1] = max wave speed of solve s
 void launch_batch_gather(const BatchSolve* d, int nsolves, float* out, cudaStream_t s);
 // l2[s] = sqrt(mean over solve s's cells of (d rho / dt)^2), from the stage-0 residual;
 // part holds one double per tile.  Summation order depends only on the solve's own grid.
-void launch_batch_residual_norm(const BatchSolve* d, int nsolves, int total_tiles, double* part, double* l2,
-                                cudaStream_t s);
+void launch_batch_residual_norm(const BatchSolve* d, int nsolves, int total_tiles, int rows, double* part,
+                                double* l2, cudaStream_t s);
 
 // ---- full-FP64 engine (kernels_f64.cu, built with -fmad=false) ----
 // The reference-shaped engine in double on its own buffers; vertices are the solver's

@@ -15,6 +15,7 @@
 // stream alone.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <string>
@@ -47,6 +48,9 @@ struct ausm_batch {
   BatchSolve* d_solves = nullptr;
   CUtensorMap* d_maps = nullptr;  // 8 per descriptor (halo[3], plain[3], mi, mj) when tma
   bool tma = false;               // every member has tensor maps: stages load tiles by TMA
+  int rows = 16;                  // tile height of the work list
+  int tuned_rows = 0;             // height chosen by the last tuning run (0: none yet)
+  double tuned_cells = 0.0;       // the batch's cell count at that run
   int* d_err = nullptr;           // set by a TMA tile whose bounded wait gave up
   int cap = 0;  // descriptor capacity of d_solves / d_maps / d_out / d_l2
   float* d_out = nullptr;
@@ -62,7 +66,7 @@ struct ausm_batch {
 
 namespace {
 
-constexpr int kTX = 32, kTY = 16;  // tile of the batched stage kernel
+constexpr int kTX = 32;  // tile width of the batched stage kernels (height: ausm_batch::rows)
 
 int bfail(ausm_batch* b, int code, const std::string& msg) {
   ausm::set_thread_error(msg);
@@ -164,13 +168,15 @@ void relayout(ausm_batch* b) {
   int t = 0;
   b->groups.clear();
   b->tma = !b->members.empty();
-  for (ausm_solver* h : b->members) b->tma = b->tma && h->tma.ok;
+  for (ausm_solver* h : b->members) b->tma = b->tma && h->tma[0].ok && h->tma[1].ok && h->tma[2].ok;
+  if (!b->tma) b->rows = 16;
+  const int rows = b->rows;
   for (int k : b->order) {
     const ausm_solver* h = b->members[k];
     const int s = (int)b->mirror.size();
     if (b->groups.empty() || b->groups.back().scheme != h->p.scheme) b->groups.push_back({h->p.scheme, s, s, t, t});
     b->mirror.push_back(describe(h, t, maps_of(b, s)));
-    t += ((h->M + kTX - 1) / kTX) * ((h->N + kTY - 1) / kTY);
+    t += ((h->M + kTX - 1) / kTX) * ((h->N + rows - 1) / rows);
     b->groups.back().s_hi = s + 1;
     b->groups.back().t_hi = t;
   }
@@ -201,7 +207,7 @@ int sync_descriptors(ausm_batch* b) {
       std::vector<CUtensorMap> maps;
       maps.reserve(8 * b->members.size());
       for (int k : b->order) {
-        const ausm::TmaMaps& t = b->members[k]->tma;
+        const ausm::TmaMaps& t = b->members[k]->tma[ausm::tile_index(b->rows)];
         for (int q = 0; q < 3; q++) maps.push_back(t.halo[q]);
         for (int q = 0; q < 3; q++) maps.push_back(t.plain[q]);
         maps.push_back(t.mi);
@@ -230,9 +236,10 @@ void enqueue_steps(ausm_batch* b, int n) {
     const ausm_batch::Group& q = b->groups[g];
     cudaStream_t s = g == 0 ? b->st : b->aux[g - 1];
     for (int k = 0; k < n; k++) {
-      ausm::launch_batch_stage(q.scheme, 1, false, b->d_solves, q.s_lo, q.s_hi, q.t_lo, q.t_hi, k, err, s);
-      ausm::launch_batch_stage(q.scheme, 2, false, b->d_solves, q.s_lo, q.s_hi, q.t_lo, q.t_hi, k, err, s);
-      ausm::launch_batch_stage(q.scheme, 3, k == n - 1, b->d_solves, q.s_lo, q.s_hi, q.t_lo, q.t_hi, k, err, s);
+      ausm::launch_batch_stage(q.scheme, 1, false, b->d_solves, q.s_lo, q.s_hi, q.t_lo, q.t_hi, k, b->rows, err, s);
+      ausm::launch_batch_stage(q.scheme, 2, false, b->d_solves, q.s_lo, q.s_hi, q.t_lo, q.t_hi, k, b->rows, err, s);
+      ausm::launch_batch_stage(q.scheme, 3, k == n - 1, b->d_solves, q.s_lo, q.s_hi, q.t_lo, q.t_hi, k, b->rows, err,
+                               s);
     }
   }
   for (int g = 1; g < G; g++) {
@@ -241,6 +248,65 @@ void enqueue_steps(ausm_batch* b, int n) {
   }
   ausm::launch_batch_advance(b->d_solves, ns, n, b->st);
   ausm::launch_batch_gather(b->d_solves, ns, b->d_out, b->st);
+}
+
+// Tile-height autotuning of the batch (as tuned_tile_rows for one solve): for each
+// candidate height the work list is laid out again and the stage-1 launches of every
+// scheme group are timed on the members' own data (stage 1 writes only each member's
+// scratch buffer).  Runs on the first step and again when the batch's cell count has
+// changed by more than a factor of two; AUSM_TILE_ROWS fixes the height.
+int tune_rows(ausm_batch* b) {
+  double cells = 0.0;
+  for (ausm_solver* h : b->members) cells += (double)h->M * h->N;
+  if (!b->tma) return AUSM_OK;
+  int fixed = 0;
+  if (const char* e = std::getenv("AUSM_TILE_ROWS")) fixed = std::atoi(e);
+  if (const char* e = std::getenv("AUSM_AUTOTUNE"))
+    if (e[0] == '0') fixed = 16;
+  if (fixed == 8 || fixed == 16 || fixed == 32) {
+    if (b->rows != fixed) {
+      b->rows = fixed;
+      relayout(b);
+      int rc = ensure_capacity(b);
+      if (rc) return rc;
+    }
+    return AUSM_OK;
+  }
+  if (b->tuned_rows && cells <= 2.0 * b->tuned_cells && 2.0 * cells >= b->tuned_cells) return AUSM_OK;
+  const int reps = (int)std::max(3.0, std::min(50.0, 4.0e6 / std::max(cells, 1.0)));
+  float best = INFINITY;
+  int best_rows = 16;
+  for (int r : {8, 16, 32}) {
+    b->rows = r;
+    relayout(b);
+    int rc = ensure_capacity(b);
+    if (!rc) rc = sync_descriptors(b);
+    if (rc) return rc;
+    auto launch = [&] {
+      for (const ausm_batch::Group& q : b->groups)
+        ausm::launch_batch_stage(q.scheme, 1, false, b->d_solves, q.s_lo, q.s_hi, q.t_lo, q.t_hi, 0, r, b->d_err,
+                                 b->st);
+    };
+    launch();
+    BCU(b, cudaEventRecord(b->e0, b->st));
+    for (int k = 0; k < reps; k++) launch();
+    BCU(b, cudaEventRecord(b->e1, b->st));
+    BCU(b, cudaEventSynchronize(b->e1));
+    BCU(b, cudaGetLastError());
+    float ms = 0.0f;
+    BCU(b, cudaEventElapsedTime(&ms, b->e0, b->e1));
+    if (ms < best) {
+      best = ms;
+      best_rows = r;
+    }
+  }
+  b->rows = best_rows;
+  relayout(b);
+  int rc = ensure_capacity(b);
+  if (rc) return rc;
+  b->tuned_rows = best_rows;
+  b->tuned_cells = cells;
+  return AUSM_OK;
 }
 
 int run_steps(ausm_batch* b, int n) {
@@ -387,6 +453,8 @@ int ausm_batch_step(ausm_batch* b, int n, float* dt_wave) {
   if (ns == 0 || n == 0) return AUSM_OK;
   for (ausm_solver* h : b->members)
     BNEED(b, h->has_grid && h->has_state, AUSM_ERR_STATE, "a member lost its grid or state");
+  rc = tune_rows(b);
+  if (rc) return rc;
   rc = sync_descriptors(b);
   if (rc) return rc;
   rc = run_steps(b, n);
@@ -426,8 +494,9 @@ int ausm_batch_residual_l2(ausm_batch* b, double* l2) {
   rc = sync_descriptors(b);
   if (rc) return rc;
   for (const ausm_batch::Group& q : b->groups)
-    ausm::launch_batch_stage(q.scheme, 0, false, b->d_solves, q.s_lo, q.s_hi, q.t_lo, q.t_hi, 0, nullptr, b->st);
-  ausm::launch_batch_residual_norm(b->d_solves, ns, b->total_tiles, b->d_part, b->d_l2, b->st);
+    ausm::launch_batch_stage(q.scheme, 0, false, b->d_solves, q.s_lo, q.s_hi, q.t_lo, q.t_hi, 0, b->rows, nullptr,
+                             b->st);
+  ausm::launch_batch_residual_norm(b->d_solves, ns, b->total_tiles, b->rows, b->d_part, b->d_l2, b->st);
   BCU(b, cudaGetLastError());
   BCU(b, cudaMemcpyAsync(b->h_l2, b->d_l2, ns * sizeof(double), cudaMemcpyDeviceToHost, b->st));
   BCU(b, cudaStreamSynchronize(b->st));

@@ -1,18 +1,19 @@
 // Batched stage kernel: one launch per RK stage and scheme advances every solve of that
 // scheme in a batch of independent O-grids of any sizes (stage 0: residual only).  The
-// work list is the concatenation of all solves' 32 x 16 tiles, grouped by scheme; each
+// work list is the concatenation of all solves' 32 x TY tiles, grouped by scheme; each
 // CTA takes one work item, finds its solve by binary search over the solves'
 // first-tile offsets, and runs the same tile compute as the single-solve kernel
 // (stage_tile.cuh) with that solve's buffers, constants and dt; with TMA (every solve
-// has tensor maps) its boxes are loaded through the solve's maps (tile_tma.cuh).  The scheme is a
-// template parameter: a run-time scheme switch inside one kernel holds all three flux
-// variants' registers at once and spills at the 64-register budget of 4 CTAs per SM.
-// One CTA per item rather than a persistent grid-stride loop: the hardware block
-// scheduler hands out items dynamically, and on B200 the persistent form ran 8% slower.
-// Each solve's dt comes from its own max wave speed, so a solve's arithmetic is the
-// same alone or in any batch.  The buffer rotation lives in the descriptors (cur,
-// advanced on the device after a step sequence), so one captured CUDA graph of n steps
-// can be replayed for any number of rounds.
+// has tensor maps) its boxes are loaded through the solve's maps (tile_tma.cuh).  The
+// tile height TY (8, 16 or 32) is chosen per batch by the autotuner (batch.cu).  The
+// scheme is a template parameter: a run-time scheme switch inside one kernel holds all
+// three flux variants' registers at once and spills at the 64-register budget.  One
+// CTA per item rather than a persistent grid-stride loop: the hardware block scheduler
+// hands out items dynamically, and on B200 the persistent form ran 8% slower.  Each
+// solve's dt comes from its own max wave speed, so a solve's arithmetic is the same
+// alone or in any batch.  The buffer rotation lives in the descriptors (cur, advanced
+// on the device after a step sequence), so one captured CUDA graph of n steps can be
+// replayed for any number of rounds.
 #include <algorithm>
 
 #include "stage_tile.cuh"
@@ -20,10 +21,6 @@
 
 namespace ausm {
 using namespace tile;
-
-#ifndef AUSM_BATCH_MIN_BLOCKS
-#define AUSM_BATCH_MIN_BLOCKS 4
-#endif
 
 // solve owning work item `item` among descriptors [lo, hi): the last whose first tile
 // is <= item
@@ -37,14 +34,23 @@ __device__ __forceinline__ int solve_of(const BatchSolve* __restrict__ solves, i
   return lo;
 }
 
+// dynamic shared memory of the per-thread-load kernel: P, Ti, Tj
+template <int TY> struct LdgSmem {
+  static constexpr int OFF_I = (TX + 4) * (TY + 4) * 16;
+  static constexpr int OFF_J = OFF_I + TY * (TX + 1) * 16;
+  static constexpr int BYTES = OFF_J + (TY + 1) * TX * 16;
+};
+
 // One CTA per work item of one scheme group: item t0 + blockIdx.x, its solve among
-// descriptors [s_lo, s_hi).
-template <int SCHEME, int STAGE, bool EMIT>
-__global__ void __launch_bounds__(NT, AUSM_BATCH_MIN_BLOCKS)
+// descriptors [s_lo, s_hi); per-thread loads.
+template <int SCHEME, int STAGE, bool EMIT, int TY>
+__global__ void __launch_bounds__(Geo<TY>::NT, Geo<TY>::MIN_BLOCKS)
     k_batch_stage(const BatchSolve* __restrict__ solves, const int s_lo, const int s_hi, const int t0, const int rot) {
-  __shared__ float4 P[PH][PW];
-  __shared__ float4 Ti[TY][TX + 1];
-  __shared__ float4 Tj[TY + 1][TX];
+  using G = Geo<TY>;
+  extern __shared__ __align__(16) unsigned char smem_ldg[];  // P, Ti, Tj (LdgSmem<TY>)
+  float4(*P)[G::PW] = reinterpret_cast<float4(*)[G::PW]>(smem_ldg);
+  float4(*Ti)[TX + 1] = reinterpret_cast<float4(*)[TX + 1]>(smem_ldg + LdgSmem<TY>::OFF_I);
+  float4(*Tj)[TX] = reinterpret_cast<float4(*)[TX]>(smem_ldg + LdgSmem<TY>::OFF_J);
   const int tx = threadIdx.x, ty = threadIdx.y;
   const int item = t0 + blockIdx.x;
   const BatchSolve& d = solves[solve_of(solves, s_lo, s_hi, item)];
@@ -56,38 +62,21 @@ __global__ void __launch_bounds__(NT, AUSM_BATCH_MIN_BLOCKS)
   const float4* Qs = d.Q[STAGE <= 1 ? a : (STAGE == 2 ? b : c3)];
   const float4* Qn = d.Q[a];
   float4* Qo = d.Q[STAGE == 2 ? c3 : b];
-  const float4* Mi = d.Mi;
-  const float4* Mj = d.Mj;
-
-  const int ic = wrap_i(i0 + tx, M);
-  const float4 qa = tile_cell(Qs, Mj, c, M, N, ic, j0 + ty);
-  const float4 qb = tile_cell(Qs, Mj, c, M, N, ic, j0 + ty + 8);
-  int hr, hc;
-  halo_entry(tx, ty, hr, hc);
-  float4 qh = make_float4(1.0f, 0.0f, 0.0f, 1.0f);
-  if (hr >= 0) qh = tile_cell(Qs, Mj, c, M, N, wrap_i(i0 - 2 + hc, M), j0 - 2 + hr);
-  stage_faces(Mi, Mj, Ti, Tj, i0, j0, ic, M, N, tx, ty);
-  P[ty + 2][tx + 2] = to_prim<true>(qa, c.gm1);
-  P[ty + 10][tx + 2] = to_prim<true>(qb, c.gm1);
-  if (hr >= 0) P[hr][hc] = to_prim<true>(qh, c.gm1);
+  float4 qa, qb;
+  stage_tile_ldg<TY>(Qs, d.Mi, d.Mj, c, P, Ti, Tj, i0, j0, M, N, tx, ty, qa, qb);
   __syncthreads();
-
-  const FaceW w = own_weights(Ti, Tj, tx, ty);
-  faces_phase<SCHEME>(P, Ti, Tj, c, i0, j0, M, N, tx, ty);
+  const FaceW w = own_weights<TY>(Ti, Tj, tx, ty);
+  faces_phase<SCHEME, TY>(P, Ti, Tj, c, i0, j0, M, N, tx, ty);
   __syncthreads();
-
-  auto qn = [&](int h) { return __ldg(&Qn[(size_t)(j0 + ty + 8 * h) * M + i0 + tx]); };
-  uint32_t wv = combine_phase<STAGE, EMIT>(Ti, Tj, w, qa, qb, qn, Qo, *d.dt, c, i0, j0, M, N, tx, ty);
-  if constexpr (EMIT) {
-    wv = __reduce_max_sync(0xffffffffu, wv);
-    if (tx == 0) atomicMax(d.wave, wv);
-  }
+  auto qn = [&](int h) { return __ldg(&Qn[(size_t)(j0 + ty + G::NWY * h) * M + i0 + tx]); };
+  uint32_t wv = combine_phase<STAGE, EMIT, TY>(Ti, Tj, w, qa, qb, qn, Qo, *d.dt, c, i0, j0, M, N, tx, ty);
+  if constexpr (EMIT) block_max_to(d.wave, wv);
 }
 
-// TMA-staged form of k_batch_stage (stages 1-3): the tile's boxes come through the
-// solve's own tensor maps (in global memory).
-template <int SCHEME, int STAGE, bool EMIT>
-__global__ void __launch_bounds__(NT, AUSM_BATCH_MIN_BLOCKS)
+// TMA-staged form (stages 1-3): the tile's boxes come through the solve's own tensor
+// maps (in global memory, for this tile height).
+template <int SCHEME, int STAGE, bool EMIT, int TY>
+__global__ void __launch_bounds__(Geo<TY>::NT, Geo<TY>::MIN_BLOCKS)
     k_batch_stage_tma(const BatchSolve* __restrict__ solves, const int s_lo, const int s_hi, const int t0,
                       const int rot, int* __restrict__ err) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -102,8 +91,9 @@ __global__ void __launch_bounds__(NT, AUSM_BATCH_MIN_BLOCKS)
   const int s_in = STAGE == 1 ? a : (STAGE == 2 ? b : c3);
   const CUtensorMap* mp = d.maps;
   uint32_t wmax = 0u;
-  if (!tile_tma_body<SCHEME, STAGE, EMIT>(smem, &mp[s_in], &mp[3 + a], &mp[6], &mp[7], d.Q[s_in],
-                                          d.Q[STAGE == 2 ? c3 : b], d.Mi, d.Mj, *d.dt, c, M, N, i0, j0, err, wmax))
+  if (!tile_tma_body<SCHEME, STAGE, EMIT, TY>(smem, &mp[s_in], &mp[3 + a], &mp[6], &mp[7], d.Q[s_in],
+                                              d.Q[STAGE == 2 ? c3 : b], d.Mi, d.Mj, *d.dt, c, M, N, i0, j0, err,
+                                              wmax))
     return;
   if constexpr (EMIT) block_max_to(d.wave, wmax);
 }
@@ -131,6 +121,7 @@ __global__ void k_batch_gather(const BatchSolve* __restrict__ solves, int n, flo
 
 // One CTA per tile: sum of (d rho / dt)^2 over the tile's cells of the stage-0 output,
 // in a fixed order (strided per-thread sums, then a shared-memory tree).
+template <int TY>
 __global__ void __launch_bounds__(256) k_batch_tile_sumsq(const BatchSolve* __restrict__ solves, int nsolves,
                                                           double* __restrict__ part) {
   const int item = blockIdx.x;
@@ -157,12 +148,12 @@ __global__ void __launch_bounds__(256) k_batch_tile_sumsq(const BatchSolve* __re
 }
 
 // One warp per solve: lane-strided sums over the solve's tiles, then a fixed butterfly.
-__global__ void k_batch_norm(const BatchSolve* __restrict__ solves, int nsolves, const double* __restrict__ part,
-                             double* __restrict__ l2) {
+__global__ void k_batch_norm(const BatchSolve* __restrict__ solves, int nsolves, int rows,
+                             const double* __restrict__ part, double* __restrict__ l2) {
   const int s = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
   if (s >= nsolves) return;
   const BatchSolve& d = solves[s];
-  const int ntiles = d.tiles_x * ((d.N + TY - 1) / TY);
+  const int ntiles = d.tiles_x * ((d.N + rows - 1) / rows);
   double acc = 0.0;
   for (int t = lane; t < ntiles; t += 32) acc += part[d.tile0 + t];
   for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
@@ -172,11 +163,13 @@ __global__ void k_batch_norm(const BatchSolve* __restrict__ solves, int nsolves,
 void launch_batch_gather(const BatchSolve* d, int nsolves, float* out, cudaStream_t s) {
   k_batch_gather<<<(nsolves + 127) / 128, 128, 0, s>>>(d, nsolves, out);
 }
-void launch_batch_residual_norm(const BatchSolve* d, int nsolves, int total_tiles, double* part, double* l2,
-                                cudaStream_t s) {
+void launch_batch_residual_norm(const BatchSolve* d, int nsolves, int total_tiles, int rows, double* part,
+                                double* l2, cudaStream_t s) {
   if (total_tiles <= 0) return;
-  k_batch_tile_sumsq<<<total_tiles, 256, 0, s>>>(d, nsolves, part);
-  k_batch_norm<<<(nsolves + 3) / 4, 128, 0, s>>>(d, nsolves, part, l2);
+  if (rows == 8) k_batch_tile_sumsq<8><<<total_tiles, 256, 0, s>>>(d, nsolves, part);
+  else if (rows == 32) k_batch_tile_sumsq<32><<<total_tiles, 256, 0, s>>>(d, nsolves, part);
+  else k_batch_tile_sumsq<16><<<total_tiles, 256, 0, s>>>(d, nsolves, part);
+  k_batch_norm<<<(nsolves + 3) / 4, 128, 0, s>>>(d, nsolves, rows, part, l2);
 }
 
 void launch_batch_dt(BatchSolve* d, int nsolves, cudaStream_t s) {
@@ -187,38 +180,56 @@ void launch_batch_advance(BatchSolve* d, int nsolves, int steps, cudaStream_t s)
 }
 
 namespace {
-template <int SC, int ST, bool E>
+template <int SC, int ST, bool E, int TY>
 void launch_b(const BatchSolve* d, int s_lo, int s_hi, int t_lo, int t_hi, int rot, int* err, cudaStream_t s) {
+  const dim3 block(NWX, Geo<TY>::NWY);
   if constexpr (ST != 0) {
     if (err) {
       static bool attr = false;
       if (!attr) {
-        cudaFuncSetAttribute(k_batch_stage_tma<SC, ST, E>, cudaFuncAttributeMaxDynamicSharedMemorySize, T1_SMEM);
+        cudaFuncSetAttribute(k_batch_stage_tma<SC, ST, E, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             T1<TY>::SMEM);
         attr = true;
       }
-      k_batch_stage_tma<SC, ST, E><<<t_hi - t_lo, dim3(NWX, NWY), T1_SMEM, s>>>(d, s_lo, s_hi, t_lo, rot, err);
+      k_batch_stage_tma<SC, ST, E, TY><<<t_hi - t_lo, block, T1<TY>::SMEM, s>>>(d, s_lo, s_hi, t_lo, rot, err);
       return;
     }
   }
-  k_batch_stage<SC, ST, E><<<t_hi - t_lo, dim3(NWX, NWY), 0, s>>>(d, s_lo, s_hi, t_lo, rot);
+  // per-thread loads: the residual (any height) and batches without TMA (height 16)
+  if constexpr (ST == 0 || TY == 16) {
+    static bool attr = false;
+    if (!attr) {
+      cudaFuncSetAttribute(k_batch_stage<SC, ST, E, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           LdgSmem<TY>::BYTES);
+      attr = true;
+    }
+    k_batch_stage<SC, ST, E, TY><<<t_hi - t_lo, block, LdgSmem<TY>::BYTES, s>>>(d, s_lo, s_hi, t_lo, rot);
+  }
 }
-template <int SC>
+template <int SC, int TY>
 void launch_scheme(int stage, bool emit, const BatchSolve* d, int s_lo, int s_hi, int t_lo, int t_hi, int rot,
                    int* err, cudaStream_t s) {
-  if (stage == 0) launch_b<SC, 0, false>(d, s_lo, s_hi, t_lo, t_hi, rot, nullptr, s);
-  else if (stage == 1) launch_b<SC, 1, false>(d, s_lo, s_hi, t_lo, t_hi, rot, err, s);
-  else if (stage == 2) launch_b<SC, 2, false>(d, s_lo, s_hi, t_lo, t_hi, rot, err, s);
-  else if (emit) launch_b<SC, 3, true>(d, s_lo, s_hi, t_lo, t_hi, rot, err, s);
-  else launch_b<SC, 3, false>(d, s_lo, s_hi, t_lo, t_hi, rot, err, s);
+  if (stage == 0) launch_b<SC, 0, false, TY>(d, s_lo, s_hi, t_lo, t_hi, rot, nullptr, s);
+  else if (stage == 1) launch_b<SC, 1, false, TY>(d, s_lo, s_hi, t_lo, t_hi, rot, err, s);
+  else if (stage == 2) launch_b<SC, 2, false, TY>(d, s_lo, s_hi, t_lo, t_hi, rot, err, s);
+  else if (emit) launch_b<SC, 3, true, TY>(d, s_lo, s_hi, t_lo, t_hi, rot, err, s);
+  else launch_b<SC, 3, false, TY>(d, s_lo, s_hi, t_lo, t_hi, rot, err, s);
+}
+template <int TY>
+void launch_rows(int scheme, int stage, bool emit, const BatchSolve* d, int s_lo, int s_hi, int t_lo, int t_hi,
+                 int rot, int* err, cudaStream_t s) {
+  if (scheme == 0) launch_scheme<0, TY>(stage, emit, d, s_lo, s_hi, t_lo, t_hi, rot, err, s);
+  else if (scheme == 1) launch_scheme<1, TY>(stage, emit, d, s_lo, s_hi, t_lo, t_hi, rot, err, s);
+  else launch_scheme<2, TY>(stage, emit, d, s_lo, s_hi, t_lo, t_hi, rot, err, s);
 }
 }  // namespace
 
 void launch_batch_stage(int scheme, int stage, bool emit, const BatchSolve* d, int s_lo, int s_hi, int t_lo,
-                        int t_hi, int rot, int* err, cudaStream_t s) {
+                        int t_hi, int rot, int rows, int* err, cudaStream_t s) {
   if (t_hi <= t_lo) return;
-  if (scheme == 0) launch_scheme<0>(stage, emit, d, s_lo, s_hi, t_lo, t_hi, rot, err, s);
-  else if (scheme == 1) launch_scheme<1>(stage, emit, d, s_lo, s_hi, t_lo, t_hi, rot, err, s);
-  else launch_scheme<2>(stage, emit, d, s_lo, s_hi, t_lo, t_hi, rot, err, s);
+  if (rows == 8) launch_rows<8>(scheme, stage, emit, d, s_lo, s_hi, t_lo, t_hi, rot, err, s);
+  else if (rows == 32) launch_rows<32>(scheme, stage, emit, d, s_lo, s_hi, t_lo, t_hi, rot, err, s);
+  else launch_rows<16>(scheme, stage, emit, d, s_lo, s_hi, t_lo, t_hi, rot, err, s);
 }
 
 }  // namespace ausm

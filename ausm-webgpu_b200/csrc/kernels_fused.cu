@@ -49,55 +49,46 @@ namespace ausm {
 
 using namespace tile;
 
-// ---- per-thread staging, one tile per CTA ----
+// tile height of the per-thread and persistent kernels
+constexpr int TYD = 16;
+using GD = Geo<TYD>;
+
+// ---- per-thread staging, one tile per CTA (AUSM_NO_TMA=1, and the residual) ----
 template <int SCHEME, int STAGE, bool EMIT>
-__global__ void __launch_bounds__(NT, AUSM_FUSED_MIN_BLOCKS)
+__global__ void __launch_bounds__(GD::NT, AUSM_FUSED_MIN_BLOCKS)
     k_fused_stage(const float4* __restrict__ Qs, const float4* __restrict__ Qn, float4* __restrict__ Qo,
                   const float4* __restrict__ Mi, const float4* __restrict__ Mj, const float* __restrict__ dtp,
                   uint32_t* __restrict__ wave, const Consts c, const int M, const int N) {
-  __shared__ float4 P[PH][PW];
-  __shared__ float4 Ti[TY][TX + 1];
-  __shared__ float4 Tj[TY + 1][TX];
-
+  __shared__ float4 P[GD::PH][GD::PW];
+  __shared__ float4 Ti[TYD][TX + 1];
+  __shared__ float4 Tj[TYD + 1][TX];
   const int tx = threadIdx.x, ty = threadIdx.y;
-  const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY;
-  const int ic = wrap_i(i0 + tx, M);  // column of the owned cells (wrapped when i0+tx >= M)
-
-  const float4 qa = tile_cell(Qs, Mj, c, M, N, ic, j0 + ty);
-  const float4 qb = tile_cell(Qs, Mj, c, M, N, ic, j0 + ty + 8);
-  int hr, hc;
-  halo_entry(tx, ty, hr, hc);
-  float4 qh = make_float4(1.0f, 0.0f, 0.0f, 1.0f);
-  if (hr >= 0) qh = tile_cell(Qs, Mj, c, M, N, wrap_i(i0 - 2 + hc, M), j0 - 2 + hr);
-  stage_faces(Mi, Mj, Ti, Tj, i0, j0, ic, M, N, tx, ty);
-  P[ty + 2][tx + 2] = to_prim<true>(qa, c.gm1);
-  P[ty + 10][tx + 2] = to_prim<true>(qb, c.gm1);
-  if (hr >= 0) P[hr][hc] = to_prim<true>(qh, c.gm1);
+  const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TYD;
+  float4 qa, qb;
+  stage_tile_ldg<TYD>(Qs, Mi, Mj, c, P, Ti, Tj, i0, j0, M, N, tx, ty, qa, qb);
   __syncthreads();
-
-  const FaceW w = own_weights(Ti, Tj, tx, ty);
-  faces_phase<SCHEME>(P, Ti, Tj, c, i0, j0, M, N, tx, ty);
+  const FaceW w = own_weights<TYD>(Ti, Tj, tx, ty);
+  faces_phase<SCHEME, TYD>(P, Ti, Tj, c, i0, j0, M, N, tx, ty);
   __syncthreads();
-
-  auto qn = [&](int h) { return __ldg(&Qn[(size_t)(j0 + ty + 8 * h) * M + i0 + tx]); };
-  uint32_t wmax = combine_phase<STAGE, EMIT>(Ti, Tj, w, qa, qb, qn, Qo, *dtp, c, i0, j0, M, N, tx, ty);
+  auto qn = [&](int h) { return __ldg(&Qn[(size_t)(j0 + ty + GD::NWY * h) * M + i0 + tx]); };
+  uint32_t wmax = combine_phase<STAGE, EMIT, TYD>(Ti, Tj, w, qa, qb, qn, Qo, *dtp, c, i0, j0, M, N, tx, ty);
   if constexpr (EMIT) block_max_to(wave, wmax);
 }
 
-// ---- persistent TMA-staged version ----
+// ---- persistent TMA-staged version (AUSM_TMA_MODE=persistent) ----
 namespace {
+using LD = T1<TYD>;
 // dynamic shared memory layout of the persistent kernel (offsets multiples of 128 B);
 // buffers 0/1 alternate
-constexpr int BUF_BYTES = r128(SQ_BYTES) + r128(SI_BYTES) + r128(SJ_BYTES);
-constexpr int OFF_BUF0 = 0, OFF_BUF1 = BUF_BYTES;
-constexpr int OFF_I = r128(SQ_BYTES), OFF_J = OFF_I + r128(SI_BYTES);  // within a buffer
+constexpr int BUF_BYTES = r128(LD::SQ) + r128(LD::SI) + r128(LD::SJ);
+constexpr int OFF_I = r128(LD::SQ), OFF_J = OFF_I + r128(LD::SI);  // within a buffer
 constexpr int OFF_N = 2 * BUF_BYTES;
-constexpr int OFF_BAR = OFF_N + r128(SN_BYTES);
+constexpr int OFF_BAR = OFF_N + r128(LD::SN);
 constexpr int TMA_SMEM = OFF_BAR + 128 + 128;  // + alignment slack
 }  // namespace
 
 template <int SCHEME, int STAGE, bool EMIT>
-__global__ void __launch_bounds__(NT, AUSM_TMA_MIN_BLOCKS)
+__global__ void __launch_bounds__(GD::NT, AUSM_TMA_MIN_BLOCKS)
     k_fused_stage_tma(const __grid_constant__ TmaMapsLaunch tm, const float4* __restrict__ Qs,
                       float4* __restrict__ Qo, const float4* __restrict__ Mi, const float4* __restrict__ Mj,
                       const float* __restrict__ dtp, uint32_t* __restrict__ wave, int* __restrict__ err,
@@ -105,7 +96,7 @@ __global__ void __launch_bounds__(NT, AUSM_TMA_MIN_BLOCKS)
   extern __shared__ __align__(128) unsigned char smem_raw[];
   // TMA destinations need 16-byte (we keep 128-byte) alignment of the dynamic region
   unsigned char* smem = smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u);
-  auto SQ = [&](int b) { return reinterpret_cast<float4(*)[PW]>(smem + b * BUF_BYTES); };
+  auto SQ = [&](int b) { return reinterpret_cast<float4(*)[GD::PW]>(smem + b * BUF_BYTES); };
   auto SI = [&](int b) { return reinterpret_cast<float4(*)[TX + 1]>(smem + b * BUF_BYTES + OFF_I); };
   auto SJ = [&](int b) { return reinterpret_cast<float4(*)[TX]>(smem + b * BUF_BYTES + OFF_J); };
   float4(*SN)[TX] = reinterpret_cast<float4(*)[TX]>(smem + OFF_N);
@@ -121,8 +112,8 @@ __global__ void __launch_bounds__(NT, AUSM_TMA_MIN_BLOCKS)
   __syncthreads();
 
   auto issue_tile = [&](int t, int buf) {  // thread 0 only
-    const int i0 = (t % tilesX) * TX, j0 = (t / tilesX) * TY;
-    mbar_expect_tx(&bars[buf], SQ_BYTES + SI_BYTES + SJ_BYTES);
+    const int i0 = (t % tilesX) * TX, j0 = (t / tilesX) * TYD;
+    mbar_expect_tx(&bars[buf], LD::SQ + LD::SI + LD::SJ);
     tma_load_2d(SQ(buf), &tm.qs, 4 * (i0 - 2), j0 - 2, &bars[buf]);
     tma_load_2d(SI(buf), &tm.mi, 4 * i0, j0, &bars[buf]);
     tma_load_2d(SJ(buf), &tm.mj, 4 * i0, j0, &bars[buf]);
@@ -134,8 +125,6 @@ __global__ void __launch_bounds__(NT, AUSM_TMA_MIN_BLOCKS)
   // `phase` the parity of its outstanding phase
   unsigned pending = 0u, phase = 0u;
   bool failed = false;
-  int hr, hc;
-  halo_entry(tx, ty, hr, hc);
 
   if (tid == 0 && blockIdx.x < numTiles) {
     issue_tile(blockIdx.x, 0);
@@ -144,11 +133,11 @@ __global__ void __launch_bounds__(NT, AUSM_TMA_MIN_BLOCKS)
   int k = 0;
   for (int t = blockIdx.x; t < numTiles; t += gridDim.x, ++k) {
     const int b = k & 1;
-    const int i0 = (t % tilesX) * TX, j0 = (t / tilesX) * TY;
+    const int i0 = (t % tilesX) * TX, j0 = (t / tilesX) * TYD;
     if constexpr (STAGE >= 2) {
       if (tid == 0) {  // Qn of this tile streams in during the face phase
         fence_proxy_async();
-        mbar_expect_tx(&bars[2], SN_BYTES);
+        mbar_expect_tx(&bars[2], LD::SN);
         tma_load_2d(SN, &tm.qn, 4 * i0, j0, &bars[2]);
         pending |= 4u;
       }
@@ -163,11 +152,9 @@ __global__ void __launch_bounds__(NT, AUSM_TMA_MIN_BLOCKS)
       pending &= ~(1u << b);
       phase ^= 1u << b;
     }
-    float4(*P)[PW] = SQ(b);
+    float4(*P)[GD::PW] = SQ(b);
     float4(*Ti)[TX + 1] = SI(b);
     float4(*Tj)[TX] = SJ(b);
-    // owned cells and the halo entry: fill seam columns and ghost rows, keep the owned
-    // conserved states, convert to primitives in place
     auto stage_entry = [&](int pr, int pc) {
       const int ig = i0 - 2 + pc, j = j0 - 2 + pr;
       float4 q;
@@ -177,10 +164,14 @@ __global__ void __launch_bounds__(NT, AUSM_TMA_MIN_BLOCKS)
       return q;
     };
     const float4 qa = stage_entry(ty + 2, tx + 2);
-    const float4 qb = stage_entry(ty + 10, tx + 2);
-    if (hr >= 0) stage_entry(hr, hc);
+    const float4 qb = stage_entry(ty + GD::NWY + 2, tx + 2);
+    for (int e = tid; e < GD::HALO; e += GD::NT) {
+      int hr, hc;
+      halo_entry<TYD>(e, hr, hc);
+      stage_entry(hr, hc);
+    }
     if (i0 + TX >= M && tx == 0) {  // the face column past the seam (zero-filled by the box)
-      for (int r = ty; r < TY; r += NWY)
+      for (int r = ty; r < TYD; r += GD::NWY)
         if (j0 + r < N) Ti[r][M - i0] = __ldg(&Mi[(size_t)(j0 + r) * M]);
     }
     __syncthreads();
@@ -190,8 +181,8 @@ __global__ void __launch_bounds__(NT, AUSM_TMA_MIN_BLOCKS)
       issue_tile(t + gridDim.x, b ^ 1);
       pending |= 1u << (b ^ 1);
     }
-    const FaceW w = own_weights(Ti, Tj, tx, ty);
-    faces_phase<SCHEME>(P, Ti, Tj, c, i0, j0, M, N, tx, ty);
+    const FaceW w = own_weights<TYD>(Ti, Tj, tx, ty);
+    faces_phase<SCHEME, TYD>(P, Ti, Tj, c, i0, j0, M, N, tx, ty);
     __syncthreads();
     if constexpr (STAGE >= 2) {
       bool okn = mbar_wait(&bars[2], k & 1);
@@ -204,8 +195,8 @@ __global__ void __launch_bounds__(NT, AUSM_TMA_MIN_BLOCKS)
         phase ^= 4u;
       }
     }
-    auto qn = [&](int h) { return SN[ty + 8 * h][tx]; };
-    wmax = max(wmax, combine_phase<STAGE, EMIT>(Ti, Tj, w, qa, qb, qn, Qo, dt, c, i0, j0, M, N, tx, ty));
+    auto qn = [&](int h) { return SN[ty + GD::NWY * h][tx]; };
+    wmax = max(wmax, combine_phase<STAGE, EMIT, TYD>(Ti, Tj, w, qa, qb, qn, Qo, dt, c, i0, j0, M, N, tx, ty));
     __syncthreads();  // SN and buffer b are free for reuse
   }
   if (failed) {
@@ -219,9 +210,9 @@ __global__ void __launch_bounds__(NT, AUSM_TMA_MIN_BLOCKS)
   if constexpr (EMIT) block_max_to(wave, wmax);
 }
 
-// ---- TMA-staged, one tile per CTA (the default) ----
-template <int SCHEME, int STAGE, bool EMIT>
-__global__ void __launch_bounds__(NT, AUSM_FUSED_MIN_BLOCKS)
+// ---- TMA-staged, one tile per CTA (the default; TY chosen by the autotuner) ----
+template <int SCHEME, int STAGE, bool EMIT, int TY>
+__global__ void __launch_bounds__(Geo<TY>::NT, Geo<TY>::MIN_BLOCKS)
     k_fused_tile_tma(const __grid_constant__ TmaMapsLaunch tm, const float4* __restrict__ Qs,
                      float4* __restrict__ Qo, const float4* __restrict__ Mi, const float4* __restrict__ Mj,
                      const float* __restrict__ dtp, uint32_t* __restrict__ wave, int* __restrict__ err,
@@ -229,79 +220,94 @@ __global__ void __launch_bounds__(NT, AUSM_FUSED_MIN_BLOCKS)
   extern __shared__ __align__(128) unsigned char smem_raw[];
   unsigned char* smem = smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u);
   uint32_t wmax = 0u;
-  if (!tile_tma_body<SCHEME, STAGE, EMIT>(smem, &tm.qs, &tm.qn, &tm.mi, &tm.mj, Qs, Qo, Mi, Mj, *dtp, c, M, N,
-                                          blockIdx.x * TX, blockIdx.y * TY, err, wmax))
+  if (!tile_tma_body<SCHEME, STAGE, EMIT, TY>(smem, &tm.qs, &tm.qn, &tm.mi, &tm.mj, Qs, Qo, Mi, Mj, *dtp, c, M, N,
+                                              blockIdx.x * TX, blockIdx.y * TY, err, wmax))
     return;
   if constexpr (EMIT) block_max_to(wave, wmax);
 }
 
 // ---- launchers ----
 namespace {
+template <int S, int ST, bool E, int TY>
+void launch_tile(const float4* Qs, float4* Qo, const float4* Mi, const float4* Mj, const float* dt, uint32_t* wave,
+                 const Consts& c, int M, int N, const TmaMapsLaunch* tm, int* err, cudaStream_t s) {
+  auto kern = k_fused_tile_tma<S, ST, E, TY>;
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, T1<TY>::SMEM);
+    attr = true;
+  }
+  const dim3 grid((M + TX - 1) / TX, (N + TY - 1) / TY);
+  kern<<<grid, dim3(NWX, Geo<TY>::NWY), T1<TY>::SMEM, s>>>(*tm, Qs, Qo, Mi, Mj, dt, wave, err, c, M, N);
+}
+
 template <int S, int ST, bool E>
 void launch_t(const float4* Qs, const float4* Qn, float4* Qo, const float4* Mi, const float4* Mj, const float* dt,
-              uint32_t* wave, const Consts& c, int M, int N, const TmaMapsLaunch* tm, int* err, cudaStream_t s) {
-  const int tilesX = (M + TX - 1) / TX, tilesY = (N + TY - 1) / TY;
-  static const bool per_tile = [] {
-    const char* e = std::getenv("AUSM_TMA_MODE");  // "tile" or "persistent" (A/B timing)
-    return !(e && std::string(e) == "persistent");
+              uint32_t* wave, const Consts& c, int M, int N, const TmaMapsLaunch* tm, int ty, int* err,
+              cudaStream_t s) {
+  const int tilesX = (M + TX - 1) / TX, tilesY = (N + TYD - 1) / TYD;
+  static const bool persistent = [] {
+    const char* e = std::getenv("AUSM_TMA_MODE");  // "persistent" selects the persistent kernel (A/B timing)
+    return e && std::string(e) == "persistent";
   }();
-  if (tm && ST != 0 && per_tile) {
-    auto kern = k_fused_tile_tma<S, ST, E>;
-    static bool attr = false;
-    if (!attr) {
-      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, T1_SMEM);
-      attr = true;
+  if constexpr (ST != 0) {
+    if (tm && !persistent) {
+      if (ty == 8) launch_tile<S, ST, E, 8>(Qs, Qo, Mi, Mj, dt, wave, c, M, N, tm, err, s);
+      else if (ty == 32) launch_tile<S, ST, E, 32>(Qs, Qo, Mi, Mj, dt, wave, c, M, N, tm, err, s);
+      else launch_tile<S, ST, E, 16>(Qs, Qo, Mi, Mj, dt, wave, c, M, N, tm, err, s);
+      return;
     }
-    kern<<<dim3(tilesX, tilesY), dim3(NWX, NWY), T1_SMEM, s>>>(*tm, Qs, Qo, Mi, Mj, dt, wave, err, c, M, N);
-  } else if (tm && ST != 0) {
-    static int blocks_per_sm = 0, sms = 0;
-    auto kern = k_fused_stage_tma<S, ST, E>;
-    if (!blocks_per_sm) {
-      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, TMA_SMEM);
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, kern, NT, TMA_SMEM);
-      int dev = 0;
-      cudaGetDevice(&dev);
-      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-      if (blocks_per_sm < 1) blocks_per_sm = 1;
+    if (tm) {  // persistent, TY = 16
+      static int blocks_per_sm = 0, sms = 0;
+      auto kern = k_fused_stage_tma<S, ST, E>;
+      if (!blocks_per_sm) {
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, TMA_SMEM);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, kern, GD::NT, TMA_SMEM);
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (blocks_per_sm < 1) blocks_per_sm = 1;
+      }
+      const int numTiles = tilesX * tilesY;
+      const int grid = std::min(numTiles, blocks_per_sm * sms);
+      kern<<<grid, dim3(NWX, GD::NWY), TMA_SMEM, s>>>(*tm, Qs, Qo, Mi, Mj, dt, wave, err, c, M, N, tilesX, numTiles);
+      return;
     }
-    const int numTiles = tilesX * tilesY;
-    const int grid = std::min(numTiles, blocks_per_sm * sms);
-    kern<<<grid, dim3(NWX, NWY), TMA_SMEM, s>>>(*tm, Qs, Qo, Mi, Mj, dt, wave, err, c, M, N, tilesX, numTiles);
-  } else {
-    k_fused_stage<S, ST, E><<<dim3(tilesX, tilesY), dim3(NWX, NWY), 0, s>>>(Qs, Qn, Qo, Mi, Mj, dt, wave, c, M, N);
   }
+  k_fused_stage<S, ST, E><<<dim3(tilesX, tilesY), dim3(NWX, GD::NWY), 0, s>>>(Qs, Qn, Qo, Mi, Mj, dt, wave, c, M, N);
 }
 template <int S>
 void launch_s(int stage, bool emit, const float4* Qs, const float4* Qn, float4* Qo, const float4* Mi,
               const float4* Mj, const float* dt, uint32_t* wave, const Consts& c, int M, int N,
-              const TmaMapsLaunch* tm, int* err, cudaStream_t s) {
+              const TmaMapsLaunch* tm, int ty, int* err, cudaStream_t s) {
   switch (stage) {
-    case 0: launch_t<S, 0, false>(Qs, Qn, Qo, Mi, Mj, dt, wave, c, M, N, tm, err, s); break;
-    case 1: launch_t<S, 1, false>(Qs, Qn, Qo, Mi, Mj, dt, wave, c, M, N, tm, err, s); break;
-    case 2: launch_t<S, 2, false>(Qs, Qn, Qo, Mi, Mj, dt, wave, c, M, N, tm, err, s); break;
+    case 0: launch_t<S, 0, false>(Qs, Qn, Qo, Mi, Mj, dt, wave, c, M, N, tm, ty, err, s); break;
+    case 1: launch_t<S, 1, false>(Qs, Qn, Qo, Mi, Mj, dt, wave, c, M, N, tm, ty, err, s); break;
+    case 2: launch_t<S, 2, false>(Qs, Qn, Qo, Mi, Mj, dt, wave, c, M, N, tm, ty, err, s); break;
     default:
-      if (emit) launch_t<S, 3, true>(Qs, Qn, Qo, Mi, Mj, dt, wave, c, M, N, tm, err, s);
-      else launch_t<S, 3, false>(Qs, Qn, Qo, Mi, Mj, dt, wave, c, M, N, tm, err, s);
+      if (emit) launch_t<S, 3, true>(Qs, Qn, Qo, Mi, Mj, dt, wave, c, M, N, tm, ty, err, s);
+      else launch_t<S, 3, false>(Qs, Qn, Qo, Mi, Mj, dt, wave, c, M, N, tm, ty, err, s);
   }
 }
 }  // namespace
 
 void launch_fused_stage(int scheme, int stage, bool emit, const float4* Qs, const float4* Qn, float4* Qo,
                         const float4* Mi, const float4* Mj, const float* dt, uint32_t* wave, const Consts& c, int M,
-                        int N, const TmaMapsLaunch* tm, int* err, cudaStream_t s) {
+                        int N, const TmaMapsLaunch* tm, int ty, int* err, cudaStream_t s) {
   switch (scheme) {
-    case 0: launch_s<0>(stage, emit, Qs, Qn, Qo, Mi, Mj, dt, wave, c, M, N, tm, err, s); break;
-    case 1: launch_s<1>(stage, emit, Qs, Qn, Qo, Mi, Mj, dt, wave, c, M, N, tm, err, s); break;
-    default: launch_s<2>(stage, emit, Qs, Qn, Qo, Mi, Mj, dt, wave, c, M, N, tm, err, s); break;
+    case 0: launch_s<0>(stage, emit, Qs, Qn, Qo, Mi, Mj, dt, wave, c, M, N, tm, ty, err, s); break;
+    case 1: launch_s<1>(stage, emit, Qs, Qn, Qo, Mi, Mj, dt, wave, c, M, N, tm, ty, err, s); break;
+    default: launch_s<2>(stage, emit, Qs, Qn, Qo, Mi, Mj, dt, wave, c, M, N, tm, ty, err, s); break;
   }
 }
 
-// Tensor maps of the TMA kernel: state buffers as 2-D float tensors of 4M x N
-// (row pitch 16 M bytes) with the halo box 144 x 20 and the Qn box 128 x 16; face
-// records Mi as 4M x N with the box 132 x 16, Mj as 4M x (N+1) with the box 128 x 17.
-// Every box's row is a multiple of 16 bytes and every x coordinate a multiple of 4
-// floats (16 bytes).
-bool encode_tma_maps(const float4* const Q[3], const float4* Mi, const float4* Mj, int M, int N, TmaMaps* out) {
+// Tensor maps of the TMA kernels for tile height ty: state buffers as 2-D float tensors
+// of 4M x N (row pitch 16 M bytes) with the halo box 144 x (ty+4) and the Qn box
+// 128 x ty; face records Mi as 4M x N with the box 132 x ty, Mj as 4M x (N+1) with the
+// box 128 x (ty+1).  Every box's row is a multiple of 16 bytes and every x coordinate a
+// multiple of 4 floats (16 bytes).
+bool encode_tma_maps(const float4* const Q[3], const float4* Mi, const float4* Mj, int M, int N, int ty,
+                     TmaMaps* out) {
   out->ok = false;
   using Encode = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
                               const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
@@ -325,12 +331,13 @@ bool encode_tma_maps(const float4* const Q[3], const float4* Mi, const float4* M
                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
   };
+  const cuuint32_t bty = (cuuint32_t)ty;
   for (int b = 0; b < 3; b++) {
-    if (!enc(&out->halo[b], Q[b], 4ull * M, N, 16ull * M, 4 * PW, PH)) return false;
-    if (!enc(&out->plain[b], Q[b], 4ull * M, N, 16ull * M, 4 * TX, TY)) return false;
+    if (!enc(&out->halo[b], Q[b], 4ull * M, N, 16ull * M, 4 * (TX + 4), bty + 4)) return false;
+    if (!enc(&out->plain[b], Q[b], 4ull * M, N, 16ull * M, 4 * TX, bty)) return false;
   }
-  if (!enc(&out->mi, Mi, 4ull * M, N, 16ull * M, 4 * (TX + 1), TY)) return false;
-  if (!enc(&out->mj, Mj, 4ull * M, N + 1, 16ull * M, 4 * TX, TY + 1)) return false;
+  if (!enc(&out->mi, Mi, 4ull * M, N, 16ull * M, 4 * (TX + 1), bty)) return false;
+  if (!enc(&out->mj, Mj, 4ull * M, N + 1, 16ull * M, 4 * TX, bty + 1)) return false;
   out->ok = true;
   return true;
 }

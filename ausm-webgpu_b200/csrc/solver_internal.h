@@ -39,7 +39,8 @@ struct ausm_solver {
   double* parts = nullptr;  // 2 * kMaxParts per-block partial sums
   uint32_t* move = nullptr;
   int* err_flag = nullptr;  // set by a kernel whose bounded wait gave up
-  ausm::TmaMaps tma;
+  ausm::TmaMaps tma[3];  // per tile height kTileHeights[k]
+  int tile_rows = 0;      // tile height of the TMA stage kernel; 0 until tuned
   float* h_dt = nullptr;
   uint32_t* h_wave = nullptr;
   double* h_acc = nullptr;
@@ -52,4 +53,9 @@ void make_consts(ausm_solver* h);
 // Inflow speed update of a ramped start after n steps (main.js:779), api.cu.
 void ramp_after_steps(ausm_solver* h, int n);
 void set_thread_error(const std::string& msg);
+// Tile height for h's fused steps: AUSM_TILE_ROWS, the process-wide tuning cache for
+// (M, N, scheme), or a tuning run (api.cu).  Enqueues work on h's stream; must not run
+// inside a stream capture.
+int tuned_tile_rows(ausm_solver* h, bool force, int* rows);
+inline int tile_index(int rows) { return rows == 8 ? 0 : (rows == 32 ? 2 : 1); }
 }  // namespace ausm

@@ -3,10 +3,14 @@
 // (flux x length of every face of the tile, each once) and the combine phase (residual
 // and RK stage combination of the two cells a thread owns).
 //
+// A tile is TX = 32 cells wide (one warp per tile row) and TY = 8, 16 or 32 cells high,
+// handled by 32 x TY/2 threads; thread (tx, ty) owns cells (tx, ty) and (tx, ty + TY/2).
+// The tile height is a template parameter chosen per solve (or batch) by the autotuner.
+//
 // Geometry comes from the FP64-computed face records (k_metrics_d): Mi[j][i] =
 // (nx, ny, len, 1/A) of the face left of cell (i, j), Mj[j][i] = (nx, ny, len, W) of
 // the face below it, W the cell's wave-speed factor.  A tile stages the records of its
-// faces in shared memory (Ti: 16 rows x 33 faces, Tj: 17 rows x 32 faces); the face
+// faces in shared memory (Ti: TY rows x 33 faces, Tj: TY+1 rows x 32 faces); the face
 // phase reads a face's record and overwrites it with that face's flux x length, so the
 // flux tiles share that memory.  Each face is read and written by one thread only, and
 // the thread that owns a cell computes that cell's left and lower faces, so it keeps
@@ -16,8 +20,16 @@
 
 namespace ausm {
 namespace tile {
-constexpr int TX = 32, TY = 16, NWX = 32, NWY = 8, NT = NWX * NWY;
-constexpr int PW = TX + 4, PH = TY + 4;
+constexpr int TX = 32, NWX = 32;
+
+template <int TY> struct Geo {
+  static_assert(TY == 8 || TY == 16 || TY == 32, "tile height");
+  static constexpr int NWY = TY / 2;           // warps (= tile rows per owned-cell row)
+  static constexpr int NT = NWX * NWY;         // threads
+  static constexpr int PW = TX + 4, PH = TY + 4;  // primitive tile with its 2-cell halo
+  static constexpr int HALO = 4 * TX + 4 * TY;    // halo entries (corners unused)
+  static constexpr int MIN_BLOCKS = 1024 / NT;    // CTAs per SM at 64 registers per thread
+};
 
 // i in [-2, M + TX + 2) -> [0, M); the last branch only runs for M < TX + 3
 __device__ __forceinline__ int wrap_i(int i, int M) {
@@ -47,28 +59,28 @@ __device__ __forceinline__ float4 tile_cell(const float4* __restrict__ Qs, const
   return make_float4(1.0f, 0.0f, 0.0f, 1.0f);  // beyond the far field: never read by a valid face
 }
 
-// halo entry of thread (tx, ty): warps 0-3 take primitive rows 0, 1, TY+2, TY+3
-// (columns 2..TX+1), warps 4-5 columns 0, 1, TX+2, TX+3 (rows 2..TY+1)
-__device__ __forceinline__ void halo_entry(int tx, int ty, int& hr, int& hc) {
-  hr = -1;
-  hc = -1;
-  if (ty < 4) {
-    hr = ty < 2 ? ty : TY + ty;
-    hc = tx + 2;
-  } else if (ty < 6) {
-    int k = (ty - 4) * 32 + tx;  // 0..63
-    int sel = k >> 4;            // 0..3
+// Halo entry k of the primitive tile (k < HALO): first the rows 0, 1, TY+2, TY+3
+// (columns 2..TX+1), then the columns 0, 1, TX+2, TX+3 (rows 2..TY+1).
+template <int TY> __device__ __forceinline__ void halo_entry(int k, int& hr, int& hc) {
+  if (k < 4 * TX) {
+    const int r = k / TX;
+    hr = r < 2 ? r : TY + r;
+    hc = 2 + k % TX;
+  } else {
+    const int k2 = k - 4 * TX, sel = k2 / TY;
     hc = sel < 2 ? sel : TX + sel;
-    hr = 2 + (k & 15);
+    hr = 2 + k2 % TY;
   }
 }
 
-// Face records of the tile from global memory (per-thread loads; the TMA kernel loads
+// Face records of the tile from global memory (per-thread loads; the TMA kernels load
 // the same boxes with the tensor engine).  Ti[r][cc] = Mi[j0+r][i0+cc] (cc = TX wraps
 // through the seam), Tj[r][cc] = Mj[j0+r][i0+cc]; rows past the grid are left unset.
+template <int TY>
 __device__ __forceinline__ void stage_faces(const float4* __restrict__ Mi, const float4* __restrict__ Mj,
                                             float4 (*Ti)[TX + 1], float4 (*Tj)[TX], int i0, int j0, int ic, int M,
                                             int N, int tx, int ty) {
+  constexpr int NWY = Geo<TY>::NWY;
 #pragma unroll
   for (int r = ty; r < TY; r += NWY) {
     const int j = j0 + r;
@@ -88,22 +100,27 @@ __device__ __forceinline__ void stage_faces(const float4* __restrict__ Mi, const
 struct FaceW {
   float iA[2], W[2];
 };
+template <int TY>
 __device__ __forceinline__ FaceW own_weights(const float4 (*Ti)[TX + 1], const float4 (*Tj)[TX], int tx, int ty) {
+  constexpr int NWY = Geo<TY>::NWY;
   FaceW w;
   w.iA[0] = Ti[ty][tx].w;
-  w.iA[1] = Ti[ty + 8][tx].w;
+  w.iA[1] = Ti[ty + NWY][tx].w;
   w.W[0] = Tj[ty][tx].w;
-  w.W[1] = Tj[ty + 8][tx].w;
+  w.W[1] = Tj[ty + NWY][tx].w;
   return w;
 }
 
-// Flux x length of every face of the tile, written over the face's record.
-template <int SCHEME>
-__device__ __forceinline__ void faces_phase(const float4 (*P)[PW], float4 (*Ti)[TX + 1], float4 (*Tj)[TX],
+// Flux x length of every face of the tile, written over the face's record.  Face rows
+// ty and ty + TY/2 of each direction per thread; warp 1 also takes the right face
+// column (rows 0..TY-1), warp 0 the top face row.
+template <int SCHEME, int TY>
+__device__ __forceinline__ void faces_phase(const float4 (*P)[TX + 4], float4 (*Ti)[TX + 1], float4 (*Tj)[TX],
                                             const Consts& c, int i0, int j0, int M, int N, int tx, int ty) {
+  constexpr int NWY = Geo<TY>::NWY, PW = Geo<TY>::PW;
   const int nI = ty == 1 && tx < TY ? 3 : 2;
   for (int t = 0; t < nI; t++) {
-    const int r = t < 2 ? ty + 8 * t : tx;
+    const int r = t < 2 ? ty + NWY * t : tx;
     const int cc = t < 2 ? tx : TX;
     if (j0 + r < N && cc <= M - i0) {
       const float4 m = Ti[r][cc];
@@ -114,7 +131,7 @@ __device__ __forceinline__ void faces_phase(const float4 (*P)[PW], float4 (*Ti)[
   }
   const int nJ = ty == 0 ? 3 : 2;
   for (int t = 0; t < nJ; t++) {
-    const int r = t < 2 ? ty + 8 * t : TY;
+    const int r = t < 2 ? ty + NWY * t : TY;
     const int cc = tx;
     if (j0 + r <= N && i0 + cc < M) {
       const float4 m = Tj[r][cc];
@@ -128,15 +145,16 @@ __device__ __forceinline__ void faces_phase(const float4 (*P)[PW], float4 (*Ti)[
 // Residual and stage combination of the two owned cells from the face fluxes Fi (over
 // Ti) and Fj (over Tj); returns the max wave-speed bits of the new state when EMIT.
 // qn(h) fetches Qn of owned cell h (stages 2, 3).
-template <int STAGE, bool EMIT, class QnFetch>
+template <int STAGE, bool EMIT, int TY, class QnFetch>
 __device__ __forceinline__ uint32_t combine_phase(const float4 (*Fi)[TX + 1], const float4 (*Fj)[TX], const FaceW& w,
                                                   float4 qa, float4 qb, QnFetch qn, float4* __restrict__ Qo, float dt,
                                                   const Consts& c, int i0, int j0, int M, int N, int tx, int ty) {
+  constexpr int NWY = Geo<TY>::NWY;
   uint32_t wmax = 0u;
   const int i = i0 + tx;
 #pragma unroll
   for (int h = 0; h < 2; h++) {
-    const int r = ty + 8 * h;
+    const int r = ty + NWY * h;
     const int j = j0 + r;
     if (i < M && j < N) {
       const float4 q = h ? qb : qa;
@@ -167,6 +185,43 @@ __device__ __forceinline__ uint32_t combine_phase(const float4 (*Fi)[TX + 1], co
     }
   }
   return wmax;
+}
+
+// Per-thread staging of a whole tile (the kernels without TMA): the owned cells and the
+// halo into P (as primitives), the face records into Ti / Tj.  Returns the owned
+// conserved states.
+template <int TY>
+__device__ __forceinline__ void stage_tile_ldg(const float4* __restrict__ Qs, const float4* __restrict__ Mi,
+                                               const float4* __restrict__ Mj, const Consts& c, float4 (*P)[TX + 4],
+                                               float4 (*Ti)[TX + 1], float4 (*Tj)[TX], int i0, int j0, int M, int N,
+                                               int tx, int ty, float4& qa, float4& qb) {
+  constexpr int NWY = Geo<TY>::NWY, NT = Geo<TY>::NT, HALO = Geo<TY>::HALO;
+  const int ic = wrap_i(i0 + tx, M);
+  qa = tile_cell(Qs, Mj, c, M, N, ic, j0 + ty);
+  qb = tile_cell(Qs, Mj, c, M, N, ic, j0 + ty + NWY);
+  const int tid = ty * NWX + tx;
+  float4 qh[(HALO + NT - 1) / NT];
+#pragma unroll
+  for (int e = 0; e < (HALO + NT - 1) / NT; e++) {
+    const int k = tid + e * NT;
+    if (k < HALO) {
+      int hr, hc;
+      halo_entry<TY>(k, hr, hc);
+      qh[e] = tile_cell(Qs, Mj, c, M, N, wrap_i(i0 - 2 + hc, M), j0 - 2 + hr);
+    }
+  }
+  stage_faces<TY>(Mi, Mj, Ti, Tj, i0, j0, ic, M, N, tx, ty);
+  P[ty + 2][tx + 2] = to_prim<true>(qa, c.gm1);
+  P[ty + NWY + 2][tx + 2] = to_prim<true>(qb, c.gm1);
+#pragma unroll
+  for (int e = 0; e < (HALO + NT - 1) / NT; e++) {
+    const int k = tid + e * NT;
+    if (k < HALO) {
+      int hr, hc;
+      halo_entry<TY>(k, hr, hc);
+      P[hr][hc] = to_prim<true>(qh[e], c.gm1);
+    }
+  }
 }
 }  // namespace tile
 }  // namespace ausm

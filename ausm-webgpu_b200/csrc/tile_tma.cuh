@@ -1,6 +1,6 @@
 // TMA staging of one stage tile (one tile per CTA): the state box with its 2-cell halo
-// (36 x 20 float4), the face-record boxes (33 x 16 i-faces, 32 x 17 j-faces) and, for
-// stages 2 and 3, the Qn box (32 x 16) land in shared memory by four
+// (36 x (TY+4) float4), the face-record boxes (33 x TY i-faces, 32 x (TY+1) j-faces)
+// and, for stages 2 and 3, the Qn box (32 x TY) land in shared memory by four
 // cp.async.bulk.tensor copies (no multicast) completing on one mbarrier; the threads
 // then fill the seam columns and ghost rows the boxes cannot hold and run the tile
 // compute of stage_tile.cuh.  Used by the single-solve kernel (tensor maps as a kernel
@@ -13,31 +13,36 @@
 namespace ausm {
 namespace tile {
 
-constexpr int SQ_BYTES = PH * PW * 16;        // 11520: state box (36 x 20 float4)
-constexpr int SI_BYTES = TY * (TX + 1) * 16;  // 8448:  i-face box (33 x 16 float4)
-constexpr int SJ_BYTES = (TY + 1) * TX * 16;  // 8704:  j-face box (32 x 17 float4)
-constexpr int SN_BYTES = TY * TX * 16;        // 8192:  Qn box (32 x 16 float4)
 constexpr int r128(int x) { return (x + 127) / 128 * 128; }
-// dynamic shared memory of one tile (offsets multiples of 128 B from a 128-B aligned base)
-constexpr int T1_OFF_I = r128(SQ_BYTES), T1_OFF_J = T1_OFF_I + r128(SI_BYTES), T1_OFF_N = T1_OFF_J + r128(SJ_BYTES);
-constexpr int T1_OFF_BAR = T1_OFF_N + r128(SN_BYTES);
-constexpr int T1_SMEM = T1_OFF_BAR + 128 + 128;  // + alignment slack of the base
+
+// Box sizes and the dynamic shared memory layout of one tile (offsets multiples of
+// 128 B from a 128-B aligned base).
+template <int TY> struct T1 {
+  static constexpr int SQ = (TX + 4) * (TY + 4) * 16;  // state box
+  static constexpr int SI = TY * (TX + 1) * 16;        // i-face box
+  static constexpr int SJ = (TY + 1) * TX * 16;        // j-face box
+  static constexpr int SN = TY * TX * 16;              // Qn box
+  static constexpr int OFF_I = r128(SQ), OFF_J = OFF_I + r128(SI), OFF_N = OFF_J + r128(SJ);
+  static constexpr int OFF_BAR = OFF_N + r128(SN);
+  static constexpr int SMEM = OFF_BAR + 128 + 128;  // + alignment slack of the base
+};
 
 // Loads the tile's boxes (thread 0) and waits for them (all threads, bounded).  Returns
 // false on a timeout, after setting *err and giving the copies a second bounded wait.
-template <int STAGE>
+template <int STAGE, int TY>
 __device__ __forceinline__ bool tile_tma_load(const CUtensorMap* qs, const CUtensorMap* qn, const CUtensorMap* mi,
                                               const CUtensorMap* mj, unsigned char* smem, int i0, int j0, int tid,
                                               int* err) {
-  uint64_t* bar = reinterpret_cast<uint64_t*>(smem + T1_OFF_BAR);
+  using L = T1<TY>;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem + L::OFF_BAR);
   if (tid == 0) {
     mbar_init(bar, 1);
     mbar_fence_init();
-    mbar_expect_tx(bar, SQ_BYTES + SI_BYTES + SJ_BYTES + (STAGE >= 2 ? SN_BYTES : 0));
+    mbar_expect_tx(bar, L::SQ + L::SI + L::SJ + (STAGE >= 2 ? L::SN : 0));
     tma_load_2d(smem, qs, 4 * (i0 - 2), j0 - 2, bar);
-    tma_load_2d(smem + T1_OFF_I, mi, 4 * i0, j0, bar);
-    tma_load_2d(smem + T1_OFF_J, mj, 4 * i0, j0, bar);
-    if (STAGE >= 2) tma_load_2d(smem + T1_OFF_N, qn, 4 * i0, j0, bar);
+    tma_load_2d(smem + L::OFF_I, mi, 4 * i0, j0, bar);
+    tma_load_2d(smem + L::OFF_J, mj, 4 * i0, j0, bar);
+    if (STAGE >= 2) tma_load_2d(smem + L::OFF_N, qn, 4 * i0, j0, bar);
   }
   __syncthreads();  // barrier initialised before anyone polls it
   const bool ok = mbar_wait(bar, 0);
@@ -53,20 +58,24 @@ __device__ __forceinline__ bool tile_tma_load(const CUtensorMap* qs, const CUten
 
 // The whole stage of tile (i0, j0); wmax gets the tile's max wave-speed bits (EMIT).
 // Returns false (nothing written) when the tile's loads timed out.
-template <int SCHEME, int STAGE, bool EMIT>
+template <int SCHEME, int STAGE, bool EMIT, int TY>
 __device__ __forceinline__ bool tile_tma_body(unsigned char* smem, const CUtensorMap* qs, const CUtensorMap* qn,
                                               const CUtensorMap* mi, const CUtensorMap* mj,
                                               const float4* __restrict__ Qs, float4* __restrict__ Qo,
                                               const float4* __restrict__ Mi, const float4* __restrict__ Mj, float dt,
                                               const Consts& c, int M, int N, int i0, int j0, int* err,
                                               uint32_t& wmax) {
-  float4(*P)[PW] = reinterpret_cast<float4(*)[PW]>(smem);
-  float4(*Ti)[TX + 1] = reinterpret_cast<float4(*)[TX + 1]>(smem + T1_OFF_I);
-  float4(*Tj)[TX] = reinterpret_cast<float4(*)[TX]>(smem + T1_OFF_J);
-  float4(*SN)[TX] = reinterpret_cast<float4(*)[TX]>(smem + T1_OFF_N);
+  using L = T1<TY>;
+  constexpr int NWY = Geo<TY>::NWY, NT = Geo<TY>::NT, HALO = Geo<TY>::HALO;
+  float4(*P)[TX + 4] = reinterpret_cast<float4(*)[TX + 4]>(smem);
+  float4(*Ti)[TX + 1] = reinterpret_cast<float4(*)[TX + 1]>(smem + L::OFF_I);
+  float4(*Tj)[TX] = reinterpret_cast<float4(*)[TX]>(smem + L::OFF_J);
+  float4(*SN)[TX] = reinterpret_cast<float4(*)[TX]>(smem + L::OFF_N);
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * NWX + tx;
-  if (!tile_tma_load<STAGE>(qs, qn, mi, mj, smem, i0, j0, tid, err)) return false;
+  if (!tile_tma_load<STAGE, TY>(qs, qn, mi, mj, smem, i0, j0, tid, err)) return false;
 
+  // fill seam columns and ghost rows the box could not hold, keep the owned conserved
+  // states, convert to primitives in place
   auto stage_entry = [&](int pr, int pc) {
     const int ig = i0 - 2 + pc, j = j0 - 2 + pr;
     float4 q;
@@ -75,21 +84,27 @@ __device__ __forceinline__ bool tile_tma_body(unsigned char* smem, const CUtenso
     P[pr][pc] = to_prim<true>(q, c.gm1);
     return q;
   };
-  int hr, hc;
-  halo_entry(tx, ty, hr, hc);
   const float4 qa = stage_entry(ty + 2, tx + 2);
-  const float4 qb = stage_entry(ty + 10, tx + 2);
-  if (hr >= 0) stage_entry(hr, hc);
+  const float4 qb = stage_entry(ty + NWY + 2, tx + 2);
+#pragma unroll
+  for (int e = 0; e < (HALO + NT - 1) / NT; e++) {
+    const int k = tid + e * NT;
+    if (k < HALO) {
+      int hr, hc;
+      halo_entry<TY>(k, hr, hc);
+      stage_entry(hr, hc);
+    }
+  }
   if (i0 + TX >= M && tx == 0) {  // the face column past the seam (zero-filled by the box)
     for (int r = ty; r < TY; r += NWY)
       if (j0 + r < N) Ti[r][M - i0] = __ldg(&Mi[(size_t)(j0 + r) * M]);
   }
   __syncthreads();
-  const FaceW w = own_weights(Ti, Tj, tx, ty);
-  faces_phase<SCHEME>(P, Ti, Tj, c, i0, j0, M, N, tx, ty);
+  const FaceW w = own_weights<TY>(Ti, Tj, tx, ty);
+  faces_phase<SCHEME, TY>(P, Ti, Tj, c, i0, j0, M, N, tx, ty);
   __syncthreads();
-  auto qnf = [&](int h) { return SN[ty + 8 * h][tx]; };
-  wmax = combine_phase<STAGE, EMIT>(Ti, Tj, w, qa, qb, qnf, Qo, dt, c, i0, j0, M, N, tx, ty);
+  auto qnf = [&](int h) { return SN[ty + NWY * h][tx]; };
+  wmax = combine_phase<STAGE, EMIT, TY>(Ti, Tj, w, qa, qb, qnf, Qo, dt, c, i0, j0, M, N, tx, ty);
   return true;
 }
 

@@ -225,6 +225,48 @@ def run_serve_mode(ausm, cfg):
                                            "budget", "slots")}}
 
 
+def run_precision(ausm, steps, chunk=1000):
+    """The 4096 x 3072 workload advanced `steps` RK3 steps by the FP32 fused engine
+    (FP64 metrics, residual norm and forces) and by the full-FP64 engine from the same
+    grid and initial state, dt recomputed every `chunk` steps in both; errors of the
+    FP32 run against the FP64 run."""
+    import numpy as np
+    wl = dict(WORKLOAD)
+    out = {"metric": "precision study", "workload": wl["name"], "steps": steps, "chunk": chunk}
+    runs = {}
+    for engine in ("fused", "f64"):
+        s = build_solver(ausm, wl)
+        if engine != "fused":
+            s.set_engine(engine)
+        t0 = time.perf_counter()
+        done = 0
+        while done < steps:
+            n = min(chunk, steps - done)
+            s.step(n)
+            done += n
+        runs[engine] = {"seconds": time.perf_counter() - t0, "q": s.state_f64()[1:s.N + 1],
+                        "F": s.forces(with_cp=True), "l2": s.residual_l2()}
+        s.close()
+    g = 1.4
+    def prim(q):
+        rho = q[..., 0]
+        p = (q[..., 3] - 0.5 * (q[..., 1] ** 2 + q[..., 2] ** 2) / rho) * (g - 1.0)
+        return rho, p
+    r32, p32 = prim(runs["fused"]["q"])
+    r64, p64 = prim(runs["f64"]["q"])
+    def errs(a, b):
+        return {"max_rel": float(np.abs(a - b).max() / np.abs(b).max()),
+                "l2_rel": float(np.sqrt(np.mean((a - b) ** 2)) / np.sqrt(np.mean(b ** 2)))}
+    cp32, cp64 = runs["fused"]["F"]["Cp"], runs["f64"]["F"]["Cp"]
+    F32, F64 = runs["fused"]["F"], runs["f64"]["F"]
+    out.update({"rho": errs(r32, r64), "p": errs(p32, p64), "cp": errs(cp32, cp64),
+                "cl": {"f32": F32["Cl"], "f64": F64["Cl"], "rel": abs(F32["Cl"] - F64["Cl"]) / abs(F64["Cl"])},
+                "cd": {"f32": F32["Cd"], "f64": F64["Cd"], "rel": abs(F32["Cd"] - F64["Cd"]) / abs(F64["Cd"])},
+                "residual_l2": {"f32": runs["fused"]["l2"], "f64": runs["f64"]["l2"]},
+                "seconds": {"f32": runs["fused"]["seconds"], "f64": runs["f64"]["seconds"]}})
+    return out
+
+
 def batch_specs(cfg):
     import numpy as np
     rng = np.random.default_rng(cfg["seed"])
@@ -404,9 +446,11 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--small", action="store_true", help="512x384 grid (profiling and quick checks)")
-    ap.add_argument("--mode", default="step", choices=["step", "batch", "serve"],
+    ap.add_argument("--mode", default="step", choices=["step", "batch", "serve", "precision"],
                     help="step: the 4096x3072 step (headline line, with the batched measurement "
-                         "attached); batch: the batched measurement alone; serve: the served stream")
+                         "attached); batch: the batched measurement alone; serve: the served stream; "
+                         "precision: FP32 against FP64 on the 4096x3072 workload")
+    ap.add_argument("--precision-steps", type=int, default=100000)
     ap.add_argument("--serve-requests", type=int, default=SERVE["requests"])
     ap.add_argument("--serve-rate", type=float, default=SERVE["rate"])
     ap.add_argument("--serve-max-steps", type=int, default=SERVE["max_steps"])
@@ -428,6 +472,11 @@ def main():
     ausm.set_device(local_rank)
     if args.mode == "batch":
         res = run_batched(ausm, BATCH, args.warmup)
+        if rank == 0:
+            print(json.dumps(res))
+        return 0
+    if args.mode == "precision":
+        res = run_precision(ausm, args.precision_steps)
         if rank == 0:
             print(json.dumps(res))
         return 0

@@ -187,6 +187,13 @@ int ausm_synchronize(ausm_solver* h);
 /* Device-timed loop for benchmarks: `reps` calls of step(n) bracketed by CUDA events
  * on the handle's stream; ms_out gets the elapsed device time of all of them. */
 int ausm_time_steps(ausm_solver* h, int n, int reps, float* ms_out);
+/* Tile-height autotuner of the fused engine (no counterpart in the reference): times
+ * the TMA stage kernel for tiles of 32 x 8, 32 x 16 and 32 x 32 cells on this solve's
+ * grid and state and keeps the fastest for its steps (cached per M, N and scheme for the
+ * process; force = 1 re-measures).  The first ausm_step of an untuned solve runs it
+ * implicitly, so call it before capturing steps in a CUDA graph.  AUSM_TILE_ROWS=8|16|32
+ * fixes the height, AUSM_AUTOTUNE=0 keeps 16.  *rows gets the height in use. */
+int ausm_autotune(ausm_solver* h, int force, int* rows);
 
 /* ---- batches: many solves advanced together (no counterpart in the reference) ----
  * The reference steps one grid per page.  A batch steps any number of independent

@@ -198,3 +198,26 @@ def test_batch_errors(grids):
         assert e.value.code == _lib.ERR_STATE
     s.close()
     t.close()
+
+
+def test_batch_tile_heights_bit_identical(grids, monkeypatch):
+    """The batch laid out with 8-, 16- and 32-row tiles gives the same state bits (the
+    residual norm sums per tile, so its rounding follows the tiling)."""
+    from ausm import Batch
+    out = {}
+    for rows in ("8", "16", "32"):
+        monkeypatch.setenv("AUSM_TILE_ROWS", rows)
+        sol = [make(k, grids) for k in range(len(SPECS))]
+        with Batch() as b:
+            for s in sol:
+                b.add(s)
+            for n in FRAMES:
+                b.step(n)
+            l2 = b.residual_l2()
+        out[rows] = ([s.state() for s in sol], l2)
+        for s in sol:
+            s.close()
+    for rows in ("8", "32"):
+        for a, c in zip(out[rows][0], out["16"][0]):
+            np.testing.assert_array_equal(a, c)
+        np.testing.assert_allclose(out[rows][1], out["16"][1], rtol=1e-12)

@@ -172,3 +172,36 @@ def test_symmetric_airfoil_zero_lift():
     f = s.forces()
     assert abs(f["Cl"]) < 1e-3 * max(abs(f["Cd"]), 1e-3)
     s.close()
+
+
+@pytest.mark.parametrize("name", ["run_slau2_m05_a2_fs", "run_slau_m6_odd", "run_ausmup_m8_a0_fs"])
+def test_tile_heights_bit_identical(golden, name, monkeypatch):
+    """Each face is evaluated once from the same inputs whatever the tiling, so the three
+    tile heights of the TMA stage kernel give the same bits; the autotuner only picks the
+    fastest."""
+    out = {}
+    for rows in ("8", "16", "32"):
+        monkeypatch.setenv("AUSM_TILE_ROWS", rows)
+        s, M, N = make_solver(golden, name, "fused")
+        assert s.autotune() == int(rows)
+        for n in golden[f"{name}/frames"]:
+            s.step(int(n))
+        out[rows] = s.state()
+        s.close()
+    np.testing.assert_array_equal(out["8"], out["16"])
+    np.testing.assert_array_equal(out["32"], out["16"])
+
+
+def test_autotune_picks_a_height():
+    from ausm import Solver
+    s = Solver(512, 384)
+    s.set_body_naca4(2412, 0.3, -0.7)
+    s.set_outer_rect(1.5)
+    s.generate_grid(100, "multicolor")
+    s.set_params(**lib_kwargs(dict(mach=0.8, aoa_deg=2.0)))
+    s.prepare_state("freestream")
+    assert s.autotune(force=True) in (8, 16, 32)
+    q0 = s.state()
+    s.autotune(force=True)  # tuning writes only the scratch buffer
+    np.testing.assert_array_equal(s.state(), q0)
+    s.close()
