@@ -112,6 +112,7 @@ struct ausm_server {
   std::deque<Req*> queue;
   std::vector<Req*> active;  // in batch member order
   int retiring = 0;          // finished members whose forces / teardown are in progress
+  int admitting = 0;         // requests taken off the queue whose admission is in progress
   std::unordered_map<int64_t, std::unique_ptr<Req>> reqs;
   int64_t next_id = 1;
   double in_use = 0.0, peak = 0.0, cell_updates = 0.0;
@@ -141,6 +142,7 @@ void finish(ausm_server* s, Req* q, int state, int stop) {
     q->h = nullptr;
   }
   std::lock_guard<std::mutex> lk(s->mu);
+  if (q->state == AUSM_REQ_QUEUED && q->charged) s->admitting--;  // its admission failed
   q->state = state;
   q->stop = stop;
   q->t_done = Clock::now();
@@ -191,6 +193,7 @@ bool admit(ausm_server* s, Req* q) {
   q->state = AUSM_REQ_RUNNING;
   q->t_admit = Clock::now();
   s->admitted++;
+  s->admitting--;
   s->active.push_back(q);
   return true;
 }
@@ -247,6 +250,7 @@ int pump_round(ausm_server* s, int* remaining) {
       s->queue.pop_front();
       s->in_use += f->bytes;
       f->charged = true;
+      s->admitting++;  // neither queued nor active until admit() ends
       if (s->in_use > s->peak) s->peak = s->in_use;
       q = f;
     }
@@ -304,7 +308,7 @@ int pump_round(ausm_server* s, int* remaining) {
     for (auto& d : done) retire(s, d.first, d.second);
   }
   std::lock_guard<std::mutex> lk(s->mu);
-  if (remaining) *remaining = (int)(s->queue.size() + s->active.size()) + s->retiring;
+  if (remaining) *remaining = (int)(s->queue.size() + s->active.size()) + s->retiring + s->admitting;
   s->cv.notify_all();
   return AUSM_OK;
 }
@@ -493,7 +497,7 @@ int ausm_server_drain(ausm_server* s, double timeout_ms) {
   }
   if (worker) {
     std::unique_lock<std::mutex> lk(s->mu);
-    auto idle = [&] { return s->queue.empty() && s->active.empty() && s->retiring == 0; };
+    auto idle = [&] { return s->queue.empty() && s->active.empty() && s->retiring == 0 && s->admitting == 0; };
     if (timeout_ms < 0) s->cv.wait(lk, idle);
     else if (!s->cv.wait_until(lk, t_end, idle)) return AUSM_ERR_TIMEOUT;
     return AUSM_OK;

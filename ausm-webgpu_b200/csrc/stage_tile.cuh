@@ -125,8 +125,7 @@ __device__ __forceinline__ void faces_phase(const float4 (*P)[TX + 4], float4 (*
     if (j0 + r < N && cc <= M - i0) {
       const float4 m = Ti[r][cc];
       const float4* b = &P[r + 2][cc];
-      float4 f = face_flux<SCHEME, true>(b[0], b[1], b[2], b[3], m.x, m.y, c);
-      Ti[r][cc] = make_float4(f.x * m.z, f.y * m.z, f.z * m.z, f.w * m.z);
+      Ti[r][cc] = face_flux_len<SCHEME>(b[0], b[1], b[2], b[3], m.x, m.y, m.z, c);
     }
   }
   const int nJ = ty == 0 ? 3 : 2;
@@ -136,8 +135,7 @@ __device__ __forceinline__ void faces_phase(const float4 (*P)[TX + 4], float4 (*
     if (j0 + r <= N && i0 + cc < M) {
       const float4 m = Tj[r][cc];
       const float4* b = &P[r][cc + 2];
-      float4 f = face_flux<SCHEME, true>(b[0], b[PW], b[2 * PW], b[3 * PW], m.x, m.y, c);
-      Tj[r][cc] = make_float4(f.x * m.z, f.y * m.z, f.z * m.z, f.w * m.z);
+      Tj[r][cc] = face_flux_len<SCHEME>(b[0], b[PW], b[2 * PW], b[3 * PW], m.x, m.y, m.z, c);
     }
   }
 }

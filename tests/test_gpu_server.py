@@ -124,3 +124,19 @@ def test_plain_path_matches(alone):
             assert d["state"] == _lib.REQ_DONE and d["steps"] == a["steps"] and d["stop"] == a["stop"]
             scale = np.abs(a["Cp"]).max()
             assert np.abs(d["Cp"] - a["Cp"]).max() <= 1e-6 * scale
+
+
+def test_plain_worker_drain_waits_for_admissions():
+    """One slot and a worker thread: every request is admitted while nothing else is
+    active, so drain must not mistake a request in admission for an idle server."""
+    import ausm
+    from ausm import _lib
+    with ausm.Server(16e9, chunk_steps=CHUNK, plain=True) as s:
+        s.start()
+        ids = [s.submit(req(k % 5, max_steps=100)) for k in range(8)]
+        s.drain(timeout_s=300)
+        for i in ids:
+            d = s.poll(i)
+            assert d["state"] == _lib.REQ_DONE and d["steps"] == 100, d
+            assert d["latency_ms"] >= d["run_ms"] > 0
+        s.stop()
