@@ -27,8 +27,8 @@ template <int TY> struct T1 {
   static constexpr int SMEM = OFF_BAR + 128 + 128;  // + alignment slack of the base
 };
 
-// Loads the tile's boxes (thread 0) and waits for them (all threads, bounded).  Returns
-// false on a timeout, after setting *err and giving the copies a second bounded wait.
+// Loads the tile's boxes and waits for them (thread 0 issues and polls, bounded; the
+// other threads wait at the CTA barrier).  Returns false on a timeout, after setting *err and giving the copies a second bounded wait.
 template <int STAGE, int TY>
 __device__ __forceinline__ bool tile_tma_load(const CUtensorMap* qs, const CUtensorMap* qn, const CUtensorMap* mi,
                                               const CUtensorMap* mj, unsigned char* smem, int i0, int j0, int tid,
@@ -44,8 +44,12 @@ __device__ __forceinline__ bool tile_tma_load(const CUtensorMap* qs, const CUten
     tma_load_2d(smem + L::OFF_J, mj, 4 * i0, j0, bar);
     if (STAGE >= 2) tma_load_2d(smem + L::OFF_N, qn, 4 * i0, j0, bar);
   }
-  __syncthreads();  // barrier initialised before anyone polls it
-  const bool ok = mbar_wait(bar, 0);
+  // Thread 0 alone polls the barrier (bounded); the other threads wait at the CTA
+  // barrier, which issues no instructions while the boxes land, so the other CTAs on
+  // the SM keep the issue slots.  The mbarrier wait acquires the async-proxy writes
+  // for thread 0 and the CTA barrier passes them on to the rest.
+  bool ok = true;
+  if (tid == 0) ok = mbar_wait(bar, 0);
   if (__syncthreads_or(!ok)) {
     if (tid == 0) {
       atomicExch(err, 1);
