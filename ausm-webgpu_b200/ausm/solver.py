@@ -180,11 +180,16 @@ class Solver:
         self._c(lib().ausm_max_wave_speed(self.h, C.byref(w)))
         return w.value
 
-    def forces(self, with_cp: bool = False):
+    def forces(self, with_cp: bool = False, chord: float | None = None):
+        """Surface force and coefficients as the reference computes them (graphs.js:89-100:
+        Cl, Cd are force / dynamic pressure, not divided by the chord); with `chord`, also
+        the per-unit-chord coefficients Cl_c = Cl / chord, Cd_c = Cd / chord."""
         out = np.zeros(6)
         cp = np.zeros(self.M) if with_cp else None
         self._c(lib().ausm_forces(self.h, _dp(out), _dp(cp) if cp is not None else None))
         d = dict(zip(("Fx", "Fy", "F", "Cl", "Cd", "ClCd"), out.tolist()))
+        if chord is not None:
+            d["Cl_c"], d["Cd_c"] = d["Cl"] / chord, d["Cd"] / chord
         if with_cp:
             d["Cp"] = cp
         return d
@@ -374,7 +379,7 @@ class Server:
     def submit(self, r) -> int:
         i = C.c_int64()
         self._c(lib().ausm_server_submit(self.s, C.byref(r), C.byref(i)))
-        self._M[i.value] = r.M
+        self._M[i.value] = (r.M, r.chord)
         return i.value
 
     def pump(self) -> int:
@@ -393,11 +398,13 @@ class Server:
 
     def poll(self, rid: int, with_cp: bool = True) -> dict:
         res = _lib.AusmResult()
-        cp = np.full(self._M.get(rid, 0), np.nan) if with_cp else None
+        M, chord = self._M.get(rid, (0, 1.0))
+        cp = np.full(M, np.nan) if with_cp else None
         self._c(lib().ausm_server_poll(self.s, int(rid), C.byref(res),
                                        _dp(cp) if cp is not None and cp.size else None))
         d = {k: getattr(res, k) for k, _ in res._fields_ if k != "forces"}
         d.update(zip(("Fx", "Fy", "F", "Cl", "Cd", "ClCd"), list(res.forces)))
+        d["Cl_c"], d["Cd_c"] = d["Cl"] / chord, d["Cd"] / chord  # per unit chord
         if with_cp:
             d["Cp"] = cp
         return d

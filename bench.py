@@ -553,6 +553,20 @@ def main():
             cpu = {"value": cM * cN * 2 / el / 1e6, "unit": "Mcell-updates/s", "cores": threads_used(), "kind": kind,
                    "sample": f"2 RK3 steps of a {cM}x{cN} O-grid of the same flow on the host cores"}
             del obj
+            # the same on one core (a smaller sub-grid of the same flow)
+            from oracle.oracle import oracle_lib
+            L, n0 = oracle_lib(), threads_used()
+            L.orc_set_num_threads(1)
+            try:
+                kind1, M1, N1, fn1, obj1 = cpu_reference_sample(wl, None, target_s=max(2.0, args.cpu_seconds / 3), K=1)
+                t0 = time.perf_counter()
+                fn1(1)
+                el1 = time.perf_counter() - t0
+                cpu["value_1core"] = M1 * N1 / el1 / 1e6
+                cpu["sample_1core"] = f"1 RK3 step of a {M1}x{N1} O-grid of the same flow on 1 core"
+                del obj1
+            finally:
+                L.orc_set_num_threads(n0)
         except Exception as e:  # the baseline is reported, never required
             cpu = {"value": None, "unit": "Mcell-updates/s", "cores": None, "kind": None, "sample": f"failed: {e}"}
 
@@ -567,7 +581,8 @@ def main():
                 "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic",
                 "config": {"workload": wl["name"], "cells": cells, "grid": f"{M}x{N}", "engine": args.engine,
-                           "parallelism": f"replicas{world}", "l2": "inputs larger than L2 (201 MB state)",
+                           "parallelism": f"replicas{world}", "l2": ("inputs larger than L2" if cells * 16 > 126e6 else "inputs fit in L2") +
+                           f" ({cells * 16 / 1e6:.0f} MB state, {cells * 32 / 1e6:.0f} MB face records)",
                            "wall_s": wall},
                 "gpu_launches": (4 if args.engine == "fused" else 17) * args.steps, "clocks": clocks, "roofline": roofline, "cpu_baseline": cpu,
                 "e2e": e2e, "batched": batched}

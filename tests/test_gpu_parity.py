@@ -205,3 +205,60 @@ def test_autotune_picks_a_height():
     s.autotune(force=True)  # tuning writes only the scratch buffer
     np.testing.assert_array_equal(s.state(), q0)
     s.close()
+
+
+def test_converged_run_parity():
+    """The parity gate after a converged run: NACA 0012 at M 0.5, AoA 2 on a 64 x 32 grid
+    stepped until the density residual has dropped by four decades (the oracle's run
+    decides the step count); density (relative L2 of the difference) and wall Cp
+    (max difference relative to max |Cp|) of the fused engine within 1e-4 of the
+    float oracle's."""
+    from ausm import Solver
+    from oracle.oracle import Oracle, make_params
+    from oracle.geometry_ref import naca4_boundary, rectangular_outer
+    M, N = 64, 32
+    kw = dict(mach=0.5, aoa_deg=2.0, scheme="SLAU2", cfl=0.5)
+    o = Oracle(M, N, "f32")
+    v = np.zeros((N + 1, M, 2), np.float32)
+    v[0] = naca4_boundary(M, 12, 0.3, -0.7)
+    v[N] = rectangular_outer(M, 1.5)
+    o.set_vertices(v)
+    o.grid_interpolate()
+    o.grid_jacobi(500)
+    grid = o.vertices()
+    o.metrics()
+    o.set_params(make_params(**kw))
+    o.init_state(1)
+    l2_0 = o.residual_l2()
+    frame, steps = 200, 0
+    while steps < 60000:
+        o.step(frame)
+        steps += frame
+        if o.residual_l2() <= 1e-4 * l2_0:
+            break
+    assert o.residual_l2() <= 1e-4 * l2_0, "the oracle run did not converge"
+    ref = o.state()[1:N + 1].astype(np.float64)
+    ref_f = o.forces()
+    o.close()
+    # wall Cp of the oracle state: f32 pressure of the first interior row, as the library
+    w = ref[0].astype(np.float32)
+    g = np.float32(1.4)
+    rho, u, vv = w[:, 0], w[:, 1] / w[:, 0], w[:, 2] / w[:, 0]
+    p_wall = ((w[:, 3] - np.float32(0.5) * rho * (u * u + vv * vv)) * (g - np.float32(1.0))).astype(np.float64)
+    speed = kw["mach"] * math.sqrt(1.4 * (1.0 / 1.4) / 1.0)
+    cp_ref = (p_wall - 1.0 / 1.4) / (0.5 * speed * speed)
+    s = Solver(M, N)
+    s.set_vertices(grid)
+    s.set_params(**lib_kwargs(kw))
+    s.prepare_state("freestream")
+    for _ in range(steps // frame):
+        s.step(frame)
+    q = s.state()[1:N + 1].astype(np.float64)
+    f = s.forces(with_cp=True)
+    s.close()
+    rho_l2 = np.sqrt(np.mean((q[..., 0] - ref[..., 0]) ** 2)) / np.sqrt(np.mean(ref[..., 0] ** 2))
+    assert rho_l2 <= 1e-4, f"density L2 relative difference {rho_l2:.3e} after {steps} steps"
+    dcp = np.abs(f["Cp"] - cp_ref).max() / np.abs(cp_ref).max()
+    assert dcp <= 1e-4, f"wall Cp max difference {dcp:.3e} of max |Cp|"
+    scale = max(abs(ref_f[3]), abs(ref_f[4]))
+    assert abs(f["Cl"] - ref_f[3]) <= 1e-4 * scale and abs(f["Cd"] - ref_f[4]) <= 1e-4 * scale

@@ -140,3 +140,24 @@ def test_plain_worker_drain_waits_for_admissions():
             assert d["state"] == _lib.REQ_DONE and d["steps"] == 100, d
             assert d["latency_ms"] >= d["run_ms"] > 0
         s.stop()
+
+
+def test_body_points_request_matches_naca_request():
+    """A request with the body given as points (a .dat airfoil sampled on the host) is
+    the same solve as the NACA request those points come from."""
+    import ausm
+    import numpy as np
+    from ausm.solver import lib
+    import ctypes as C
+    M = 96
+    xy = np.zeros((M, 2))
+    # the NACA 0012 points the server builds for chord 1 centred at 0 (half chord 0.5)
+    lib().ausm_naca4_points(M, 12, 0.5, 0.0, 1, xy.ctypes.data_as(C.POINTER(C.c_double)))
+    with ausm.Server(4e9, chunk_steps=CHUNK) as s:
+        a = s.submit(req(0))
+        b = s.submit(req(0, body_xy=xy))
+        s.drain()
+        ra, rb = s.poll(a), s.poll(b)
+    assert ra["state"] == 0 and rb["state"] == 0
+    np.testing.assert_array_equal(ra["Cp"], rb["Cp"])
+    assert ra["Cl_c"] == ra["Cl"]  # chord 1
