@@ -161,7 +161,6 @@ void launch_from_ref_layout(const float4* ref, float4* Qint, int M, int N, cudaS
 void launch_fill(float4* Q, float4 v, size_t n, cudaStream_t s);
 void launch_grid_init(float2* V, int M, int N, double first_spacing, cudaStream_t s);
 void launch_grid_jacobi(const float2* src, float2* dst, int M, int N, cudaStream_t s);
-void launch_grid_multicolor(float2* V, int M, int N, int color, float omega, uint32_t* move, cudaStream_t s);
 // parts: 2 * kMaxParts doubles of scratch; acc gets the sums, in a fixed order.
 // FP64 grid and face records (kernels_misc.cu): see k_metrics_d for the record layout.
 void launch_grid_init_d(double2* V, int M, int N, double first_spacing, cudaStream_t s);

@@ -81,24 +81,6 @@ __global__ void k_grid_jacobi(const float2* __restrict__ src, float2* __restrict
   if (i >= M || j < 1 || j >= N) return;
   dst[(size_t)j * M + i] = ttm_point(src, M, i, j, 1.0f);
 }
-// One colour of the multicolour Gauss-Seidel sweep: colour (i&1)*2 + (j&1); with odd M
-// the seam column i = M-1 is coloured 4 + (j&1) so no two points of a colour touch
-// (9-point stencil, periodic in i).  Records the max vertex move (float bits).
-__global__ void k_grid_multicolor(float2* __restrict__ V, int M, int N, int color, float omega, uint32_t* move) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
-  uint32_t mv = 0u;
-  if (i < M && j >= 1 && j < N) {
-    int col = ((M & 1) && i == M - 1) ? 4 + (j & 1) : (i & 1) * 2 + (j & 1);
-    if (col == color) {
-      float2 p = ttm_point(V, M, i, j, omega);
-      float2 o = V[(size_t)j * M + i];
-      float d = fmaxf(fabsf(p.x - o.x), fabsf(p.y - o.y));
-      mv = __float_as_uint(d);
-      V[(size_t)j * M + i] = p;
-    }
-  }
-  block_max_to(move, mv);
-}
 
 // ---- FP64 grid (multicolor TTM generator of the fused engine) and FP64 metrics ----
 __global__ void k_grid_init_d(double2* __restrict__ V, int M, int N, double first_spacing) {
@@ -140,7 +122,9 @@ __device__ __forceinline__ double2 ttm_point_d(const double2* __restrict__ s, in
   if (jac < 0.0) return make_double2(c.x * (1.0 - omega) + npx * omega, c.y * (1.0 - omega) + npy * omega);
   return c;
 }
-// One colour of the FP64 multicolour sweep (colouring as k_grid_multicolor).
+// One colour of the FP64 multicolour Gauss-Seidel sweep: colour (i&1)*2 + (j&1); with odd
+// M the seam column i = M-1 is coloured 4 + (j&1) so no two points of a colour touch
+// (9-point stencil, periodic in i).  Records the max vertex move (float bits).
 __global__ void k_grid_multicolor_d(double2* __restrict__ V, int M, int N, int color, double omega, uint32_t* move) {
   int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
   uint32_t mv = 0u;
@@ -291,9 +275,6 @@ void launch_grid_init(float2* V, int M, int N, double first_spacing, cudaStream_
 }
 void launch_grid_jacobi(const float2* src, float2* dst, int M, int N, cudaStream_t s) {
   k_grid_jacobi<<<grid16(M, N + 1), B16, 0, s>>>(src, dst, M, N);
-}
-void launch_grid_multicolor(float2* V, int M, int N, int color, float omega, uint32_t* move, cudaStream_t s) {
-  k_grid_multicolor<<<grid16(M, N + 1), B16, 0, s>>>(V, M, N, color, omega, move);
 }
 void launch_forces(const float4* row0, const double2* V, const Consts& c, int M, double* acc, double* parts,
                    double* cp, double q_inf, double p_inf, cudaStream_t s) {

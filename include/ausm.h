@@ -53,8 +53,9 @@ extern "C" {
 #define AUSM_OUTER_RECT 0
 #define AUSM_OUTER_CIRCLE 1
 
-/* elliptic grid iteration: the reference's Jacobi ping-pong (shaders/grid.js:33-110,
- * main.js:691-694) or multicolour Gauss-Seidel with a converged-move stop */
+/* elliptic grid iteration: the reference's Jacobi ping-pong in FP32 (shaders/grid.js:33-110,
+ * main.js:691-694), or multicolour Gauss-Seidel in FP64 with a converged-move stop (the
+ * FP64 vertices it produces give the FP64 face metrics and force integration) */
 #define AUSM_GRID_JACOBI 0
 #define AUSM_GRID_MULTICOLOR 1
 
