@@ -47,7 +47,7 @@ METRIC = "Mcell-updates/s per RK3 step"
 # NACA 4-digit bodies (camber 0-6 %, position 0.2-0.6, thickness 8-18 %), Mach U[0.1, 3],
 # AoA U[-4, 8] deg, scheme uniform over SLAU2 / SLAU / AUSM+-up, 5000 RK3 steps each from
 # a uniform freestream start, CFL 0.5; seeded.
-BATCH = dict(name="batch64_uneven_128x96-1024x768_5000steps", count=64, seed=20261203, cells_lo=128 * 96,
+BATCH = dict(name="batch64_uneven_128x96-1024x768", count=64, seed=20261203, cells_lo=128 * 96,
              cells_hi=1024 * 768, steps=5000, chunk=100, far_chords=20.0, first_spacing=1e-3, cfl=0.5,
              grid_iters=200)
 
@@ -294,13 +294,13 @@ def build_spec_solver(ausm, sp, cfg):
     return s
 
 
-def run_batched(ausm, cfg, warmup):
-    """Config: BATCH.  The same 64 solves (a) in one batch (one persistent launch per
-    RK stage over all their tiles, graph-replayed chunks of cfg['chunk'] steps) and (b)
-    by the plain path, one solve after another, each ausm_step(chunk) call launching its
-    own three stage kernels per step.  dt is recomputed every chunk steps in both.  Both
-    start from the freestream state; solves/s = 64 / elapsed.  The surface Cp of both
-    runs is compared at the end."""
+def run_batched(ausm, cfg, warmup, plain=True):
+    """Config: BATCH.  The same 64 solves (a) in one batch (one launch per RK stage and
+    scheme group over all their tiles, graph-replayed chunks of cfg['chunk'] steps) and
+    (b) by the plain path, one solve after another, each ausm_step(chunk) call launching
+    its own three stage kernels per step.  dt is recomputed every chunk steps in both.
+    Both start from the freestream state; solves/s = 64 / elapsed.  The surface Cp of
+    both runs is compared at the end.  plain=False skips (b) (profiling runs)."""
     import numpy as np
     specs = batch_specs(cfg)
     sols = [build_spec_solver(ausm, sp, cfg) for sp in specs]
@@ -322,31 +322,33 @@ def run_batched(ausm, cfg, warmup):
     for s in list(b.members):
         b.remove(s)
     b.close()
-    for s in sols:  # plain path warm-up, then the same start
-        s.step(1)
-        s.prepare_state("freestream")
-        s.synchronize()
-    t0 = time.perf_counter()
-    for s in sols:  # dt held over `chunk` steps, as in the batch
-        for _ in range(steps // chunk):
-            s.step(chunk, wait=False)
-        s.synchronize()
-    wall_p = time.perf_counter() - t0
-    cp_p = [s.forces(with_cp=True)["Cp"] for s in sols]
-    err = 0.0
-    for a, c in zip(cp_b, cp_p):
-        if np.all(np.isfinite(a)) and np.all(np.isfinite(c)):
-            err = max(err, float(np.abs(a - c).max() / max(np.abs(c).max(), 1e-30)))
+    wall_p, err = None, None
+    if plain:
+        for s in sols:  # plain path warm-up, then the same start
+            s.step(1)
+            s.prepare_state("freestream")
+            s.synchronize()
+        t0 = time.perf_counter()
+        for s in sols:  # dt held over `chunk` steps, as in the batch
+            for _ in range(steps // chunk):
+                s.step(chunk, wait=False)
+            s.synchronize()
+        wall_p = time.perf_counter() - t0
+        cp_p = [s.forces(with_cp=True)["Cp"] for s in sols]
+        err = 0.0
+        for a, c in zip(cp_b, cp_p):
+            if np.all(np.isfinite(a)) and np.all(np.isfinite(c)):
+                err = max(err, float(np.abs(a - c).max() / max(np.abs(c).max(), 1e-30)))
     for s in sols:
         s.close()
     n = len(specs)
     return {"metric": "batched solves/s", "value": n / (ms * 1e-3), "unit": "solves/s",
-            "workload": cfg["name"], "solves": n, "cells_total": cells, "steps_per_solve": steps,
+            "workload": f"{cfg['name']}_{steps}steps", "solves": n, "cells_total": cells, "steps_per_solve": steps,
             "device_ms": ms, "wall_s": wall_b, "solves_per_s_wall": n / wall_b,
-            "plain_one_launch_per_solve": {"wall_s": wall_p, "solves_per_s": n / wall_p},
-            "speedup_vs_plain": wall_p / wall_b, "cp_max_rel_diff_vs_plain": err, "diverged": diverged,
-            "mcell_updates_per_s": cells * steps / (ms * 1e-3) / 1e6,
-            "gpu_launches": (3 * chunk + 3) * (steps // chunk),
+            "plain_one_launch_per_solve": {"wall_s": wall_p, "solves_per_s": n / wall_p} if plain else None,
+            "speedup_vs_plain": wall_p / wall_b if plain else None, "cp_max_rel_diff_vs_plain": err,
+            "diverged": diverged, "mcell_updates_per_s": cells * steps / (ms * 1e-3) / 1e6,
+            "gpu_launches": (3 * chunk * len({sp["scheme"] for sp in specs}) + 3) * (steps // chunk),
             "sizes": f"{min(sp['M'] * sp['N'] for sp in specs)}..{max(sp['M'] * sp['N'] for sp in specs)} cells"}
 
 
@@ -451,6 +453,9 @@ def main():
                          "attached); batch: the batched measurement alone; serve: the served stream; "
                          "precision: FP32 against FP64 on the 4096x3072 workload")
     ap.add_argument("--precision-steps", type=int, default=100000)
+    ap.add_argument("--batch-steps", type=int, default=BATCH["steps"],
+                    help="steps per solve of the batched measurement (shorter runs for profiling only)")
+    ap.add_argument("--no-plain", action="store_true", help="batched measurement without the plain comparison")
     ap.add_argument("--serve-requests", type=int, default=SERVE["requests"])
     ap.add_argument("--serve-rate", type=float, default=SERVE["rate"])
     ap.add_argument("--serve-max-steps", type=int, default=SERVE["max_steps"])
@@ -469,9 +474,9 @@ def main():
 
     import numpy as np
     import ausm
-    ausm.set_device(local_rank)
+    ausm.set_device(local_rank % max(1, ausm.device_count()))
     if args.mode == "batch":
-        res = run_batched(ausm, BATCH, args.warmup)
+        res = run_batched(ausm, dict(BATCH, steps=args.batch_steps), args.warmup, plain=not args.no_plain)
         if rank == 0:
             print(json.dumps(res))
         return 0
