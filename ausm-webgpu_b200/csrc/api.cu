@@ -44,6 +44,7 @@ void make_consts(ausm_solver* h) {
   c.aStarK = (2.0f * c.gm1) / (g + 1.0f);
   c.ambE = inP / (g - 1.0f);
   c.gmgm1 = g / c.gm1;
+  c.minfk = c.Vinf2 / c.gammaInP;
   c.muscl = p.muscl;
   h->c = c;
   // FP64 constants from the FP64 parameters, in the oracle's operation order

@@ -26,6 +26,7 @@ struct Consts {
   float aStarK;    // (2*gm1)/(gamma+1)                   ausm.js:278
   float ambE;      // inP/(gamma-1)                       ausm.js:108
   float gmgm1;     // gamma/(gamma-1), fast enthalpy form (FAST only)
+  float minfk;     // Vinf2/gammaInP: the AUSM+-up M_inf^2 from rho_L is rho_L * minfk (FAST only)
   int muscl;
 };
 
@@ -313,8 +314,8 @@ __device__ __forceinline__ float4 face_flux(float4 L2, float4 L, float4 R, float
 
 // FAST flux x face length (the fused engines): face_flux<SCHEME, true> with the length
 // folded into the mass flux and pressure (two multiplies instead of four), no "+ 0"
-// terms (those keep the reference's sign of zero in the exact path), 1/rho guarded by
-// one max, and for SLAU / SLAU2 the pressure-split functions as the cubic
+// terms (those keep the reference's sign of zero in the exact path); for SLAU / SLAU2
+// 1/rho guarded by one max and the pressure-split functions as the cubic
 // f(M) = (M+1)^2 (2-M) / 4 of the Mach number clamped to [-1, 1], which is exactly the
 // reference's branch (|M| >= 1 gives 1 or 0, and the cubic is 1 at M = 1, 0 at M = -1,
 // within [0, 1] between, so the saturate is a no-op there).
@@ -322,8 +323,59 @@ template <int SCHEME>
 __device__ __forceinline__ float4 face_flux_len(float4 L2, float4 L, float4 R, float4 R2, float nx, float ny,
                                                 float len, const Consts& c) {
   if constexpr (SCHEME == 2) {
-    float4 f = face_flux<SCHEME, true>(L2, L, R, R2, nx, ny, c);
-    return make_float4(f.x * len, f.y * len, f.z * len, f.w * len);
+    // AUSM+-up (Liou 2006 eqs. 28-30, 69-76), as face_flux<2, true> with: M_inf^2 from
+    // rho_L as rho_L * Vinf^2 / (gamma p_inf) (one multiply for two divisions); the star
+    // speed squared used as computed (not the square of its square root); Mbar^2 =
+    // (ML^2 + MR^2) / 2 from the face Mach numbers; the K_p pressure-diffusion term only
+    // when K_p != 0 (uniform per solve; the reference's default is 0); the face length
+    // folded into the mass flux and pressure.
+    float4 Lm = L, Rm = R;
+    if (c.muscl > 0) {
+      float2 a, b;
+      muscl2_packed(lo2(L2), lo2(L), lo2(R), lo2(R2), a, b);
+      Lm.x = a.x; Lm.y = a.y; Rm.x = b.x; Rm.y = b.y;
+      muscl2_packed(hi2(L2), hi2(L), hi2(R), hi2(R2), a, b);
+      Lm.z = a.x; Lm.w = a.y; Rm.z = b.x; Rm.w = b.y;
+    }
+    const float rhoL = Lm.x, rhoR = Rm.x, pL = Lm.w, pR = Rm.w;
+    const float vxL = Lm.y, vyL = Lm.z, vxR = Rm.y, vyR = Rm.z;
+    const float uL = vxL * nx + vyL * ny, uR = vxR * nx + vyR * ny;
+    const float kL = vxL * vxL + vyL * vyL, kR = vxR * vxR + vyR * vyR;
+    const float irL = frcp<true>(rhoL), irR = frcp<true>(rhoR);
+    const float hL = c.gmgm1 * pL * irL + 0.5f * kL;
+    const float hR = c.gmgm1 * pR * irR + 0.5f * kR;
+    const float Minf2 = rhoL * c.minfk;
+    const float ht = 0.5f * (hL + hR);
+    const float as2 = fmaxf(1e-6f, c.aStarK * ht);
+    const float aStar = fsqrt<true>(as2);
+    const float aHL = as2 * frcp<true>(fmaxf(uL, aStar));
+    const float aHR = as2 * frcp<true>(fmaxf(-uR, aStar));
+    const float a = fminf(aHL, aHR);
+    const float ia = frcp<true>(a);
+    const float ML = uL * ia, MR = uR * ia;
+    const float Mbar2 = 0.5f * (ML * ML + MR * MR);
+    const float Mo2 = fminf(1.0f, fmaxf(Mbar2, Minf2));
+    const float fa = Mo2 * (2.0f - Mo2);
+    const float Mp1L = ML + 1.0f, Mp1R = MR + 1.0f, Mm1L = ML - 1.0f, Mm1R = MR - 1.0f;
+    const float M2pL = 0.25f * Mp1L * Mp1L, M2pR = 0.25f * Mp1R * Mp1R;
+    const float M2mL = -0.25f * Mm1L * Mm1L, M2mR = -0.25f * Mm1R * Mm1R;
+    const bool supL = 1.0f <= fabsf(ML), supR = 1.0f <= fabsf(MR);
+    const float M4L = supL ? fmaxf(0.0f, ML) : M2pL * (1.0f + 2.0f * M2mL);
+    const float M4R = supR ? fminf(0.0f, MR) : M2mR * (1.0f - 2.0f * M2pR);
+    float Mi = M4L + M4R;
+    if (c.Kp != 0.0f) {
+      const float rhoI = 0.5f * (rhoL + rhoR);
+      Mi -= c.Kp * frcp<true>(fa) * fmaxf(1.0f - Mbar2, 0.0f) * (pR - pL) * frcp<true>(rhoI * a * a);
+    }
+    const float alpha4 = 0.75f * (-4.0f + 5.0f * fa * fa);
+    const float P5L = supL ? (0.0f <= ML ? 1.0f : 0.0f) : M2pL * ((2.0f - ML) + alpha4 * ML * M2mL);
+    const float P5R = supR ? (0.0f <= -MR ? 1.0f : 0.0f) : M2mR * ((-2.0f - MR) - alpha4 * MR * M2pR);
+    const float P = (P5L * pL + P5R * pR) - c.Ku * P5L * P5R * (rhoL + rhoR) * fa * a * (uR - uL);
+    const float mdot = a * Mi * (Mi > 0.0f ? rhoL : rhoR);
+    const bool left = mdot > 0.0f;
+    const float ml = mdot * len, Pl = P * len;
+    const float p1 = left ? vxL : vxR, p2 = left ? vyL : vyR, p3 = left ? hL : hR;
+    return make_float4(ml, fmaf(p1, ml, nx * Pl), fmaf(p2, ml, ny * Pl), p3 * ml);
   } else {
     float4 Lm = L, Rm = R;
     if (c.muscl > 0) {
