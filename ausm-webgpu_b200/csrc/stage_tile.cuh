@@ -156,28 +156,31 @@ __device__ __forceinline__ uint32_t combine_phase(const float4 (*Fi)[TX + 1], co
     const int j = j0 + r;
     if (i < M && j < N) {
       const float4 q = h ? qb : qa;
-      const float iA = w.iA[h];
-      float4 fl = Fi[r][tx], fr = Fi[r][tx + 1], fd = Fj[r][tx], fu = Fj[r + 1][tx];
-      float4 R;
-      R.x = -(((fr.x - fl.x) + fu.x) - fd.x) * iA;
-      R.y = -(((fr.y - fl.y) + fu.y) - fd.y) * iA;
-      R.z = -(((fr.z - fl.z) + fu.z) - fd.z) * iA;
-      R.w = -(((fr.w - fl.w) + fu.w) - fd.w) * iA;
-      float4 out;
+      const float2 niA = make_float2(-w.iA[h], -w.iA[h]), m1 = make_float2(-1.0f, -1.0f);
+      const float4 fl = Fi[r][tx], fr = Fi[r][tx + 1], fd = Fj[r][tx], fu = Fj[r + 1][tx];
+      // R = -(((fr - fl) + fu) - fd) / A, two components per f32x2 operation
+      const float2 R01 = mul2(fma2(lo2(fd), m1, add2(fma2(lo2(fl), m1, lo2(fr)), lo2(fu))), niA);
+      const float2 R23 = mul2(fma2(hi2(fd), m1, add2(fma2(hi2(fl), m1, hi2(fr)), hi2(fu))), niA);
+      const float2 dt2 = make_float2(dt, dt);
+      float2 o01, o23;
       if constexpr (STAGE == 0) {  // residual only (dQ/dt)
-        out = R;
+        o01 = R01;
+        o23 = R23;
       } else if constexpr (STAGE == 1) {
-        out = make_float4(q.x + dt * R.x, q.y + dt * R.y, q.z + dt * R.z, q.w + dt * R.w);
+        o01 = fma2(dt2, R01, lo2(q));
+        o23 = fma2(dt2, R23, hi2(q));
       } else if constexpr (STAGE == 2) {
-        float4 n = qn(h);
-        out = make_float4(0.75f * n.x + 0.25f * (q.x + dt * R.x), 0.75f * n.y + 0.25f * (q.y + dt * R.y),
-                          0.75f * n.z + 0.25f * (q.z + dt * R.z), 0.75f * n.w + 0.25f * (q.w + dt * R.w));
+        const float4 n = qn(h);
+        const float2 c25 = make_float2(0.25f, 0.25f), c75 = make_float2(0.75f, 0.75f);
+        o01 = fma2(c75, lo2(n), mul2(c25, fma2(dt2, R01, lo2(q))));
+        o23 = fma2(c75, hi2(n), mul2(c25, fma2(dt2, R23, hi2(q))));
       } else {
-        float4 n = qn(h);
-        const float third = 1.0f / 3.0f;
-        out = make_float4((n.x + 2.0f * (q.x + dt * R.x)) * third, (n.y + 2.0f * (q.y + dt * R.y)) * third,
-                          (n.z + 2.0f * (q.z + dt * R.z)) * third, (n.w + 2.0f * (q.w + dt * R.w)) * third);
+        const float4 n = qn(h);
+        const float2 two = make_float2(2.0f, 2.0f), third = make_float2(1.0f / 3.0f, 1.0f / 3.0f);
+        o01 = mul2(fma2(two, fma2(dt2, R01, lo2(q)), lo2(n)), third);
+        o23 = mul2(fma2(two, fma2(dt2, R23, hi2(q)), hi2(n)), third);
       }
+      const float4 out = make_float4(o01.x, o01.y, o23.x, o23.y);
       Qo[(size_t)j * M + i] = out;
       if constexpr (EMIT) wmax = max(wmax, __float_as_uint(wave_speed_w<true>(out, w.W[h], c.gamma)));
     }
