@@ -68,6 +68,12 @@ def test_host_argument_validation():
     assert L.ausm_default_params(None) == _lib.ERR_INVALID
     with pytest.raises(_lib.AusmError):
         geometry.naca4(8, 0)
+    # grid sizes are checked before any device call
+    h = C.c_void_p()
+    assert L.ausm_create(3, 8, C.byref(h)) == _lib.ERR_INVALID and not h.value
+    assert L.ausm_create(8, 1, C.byref(h)) == _lib.ERR_INVALID
+    assert L.ausm_create(100000, 30000, C.byref(h)) == _lib.ERR_INVALID  # M (N+3) above 2e9
+    assert b"too large" in L.ausm_last_error(None)
 
 
 def _airfoil_texts():
