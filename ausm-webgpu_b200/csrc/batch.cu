@@ -273,33 +273,39 @@ int tune_rows(ausm_batch* b) {
     return AUSM_OK;
   }
   if (b->tuned_rows && cells <= 2.0 * b->tuned_cells && 2.0 * cells >= b->tuned_cells) return AUSM_OK;
-  const int reps = (int)std::max(3.0, std::min(50.0, 4.0e6 / std::max(cells, 1.0)));
-  float best = INFINITY;
-  int best_rows = 16;
-  for (int r : {8, 16, 32}) {
-    b->rows = r;
-    relayout(b);
-    int rc = ensure_capacity(b);
-    if (!rc) rc = sync_descriptors(b);
-    if (rc) return rc;
-    auto launch = [&] {
-      for (const ausm_batch::Group& q : b->groups)
-        ausm::launch_batch_stage(q.scheme, 1, false, b->d_solves, q.s_lo, q.s_hi, q.t_lo, q.t_hi, 0, r, b->d_err,
-                                 b->st);
-    };
-    launch();
-    BCU(b, cudaEventRecord(b->e0, b->st));
-    for (int k = 0; k < reps; k++) launch();
-    BCU(b, cudaEventRecord(b->e1, b->st));
-    BCU(b, cudaEventSynchronize(b->e1));
-    BCU(b, cudaGetLastError());
-    float ms = 0.0f;
-    BCU(b, cudaEventElapsedTime(&ms, b->e0, b->e1));
-    if (ms < best) {
-      best = ms;
-      best_rows = r;
+  const int reps = (int)std::max(5.0, std::min(100.0, 1.0e8 / std::max(cells, 1.0)));
+  float best_ms[3] = {INFINITY, INFINITY, INFINITY};
+  const int cand[3] = {8, 16, 32};
+  for (int round = 0; round < 2; round++)  // each candidate's best of two rounds counts
+    for (int k = 0; k < 3; k++) {
+      const int r = cand[k];
+      b->rows = r;
+      relayout(b);
+      int rc = ensure_capacity(b);
+      if (!rc) rc = sync_descriptors(b);
+      if (rc) return rc;
+      auto launch = [&] {
+        for (const ausm_batch::Group& q : b->groups)
+          ausm::launch_batch_stage(q.scheme, 1, false, b->d_solves, q.s_lo, q.s_hi, q.t_lo, q.t_hi, 0, r, b->d_err,
+                                   b->st);
+      };
+      launch();
+      BCU(b, cudaEventRecord(b->e0, b->st));
+      for (int k2 = 0; k2 < reps; k2++) launch();
+      BCU(b, cudaEventRecord(b->e1, b->st));
+      BCU(b, cudaEventSynchronize(b->e1));
+      BCU(b, cudaGetLastError());
+      float ms = 0.0f;
+      BCU(b, cudaEventElapsedTime(&ms, b->e0, b->e1));
+      best_ms[k] = std::min(best_ms[k], ms);
     }
-  }
+  int best_rows = 16;
+  float best = INFINITY;
+  for (int k = 0; k < 3; k++)
+    if (best_ms[k] < best) {
+      best = best_ms[k];
+      best_rows = cand[k];
+    }
   b->rows = best_rows;
   relayout(b);
   int rc = ensure_capacity(b);
