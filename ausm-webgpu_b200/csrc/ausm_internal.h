@@ -94,6 +94,7 @@ struct BatchSolve {
   uint32_t* wave;
   Consts c;
   int M, N, scheme, tiles_x, tile0, cur;
+  int chunk0;  // first residual-norm chunk (512 cells) of the solve
 };
 // All launches go to stream s.  rot: steps already taken since the descriptors' cur.
 // Stage 0 writes the residual dQ/dt of the current state into the solve's next buffer.
@@ -108,9 +109,10 @@ void launch_batch_advance(BatchSolve* d, int nsolves, int steps, cudaStream_t s)
 // out[2 s] = dt, out[2 s + 1] = max wave speed of solve s
 void launch_batch_gather(const BatchSolve* d, int nsolves, float* out, cudaStream_t s);
 // l2[s] = sqrt(mean over solve s's cells of (d rho / dt)^2), from the stage-0 residual;
-// part holds one double per tile.  Summation order depends only on the solve's own grid.
-void launch_batch_residual_norm(const BatchSolve* d, int nsolves, int total_tiles, int rows, double* part,
-                                double* l2, cudaStream_t s);
+// part holds one double per norm chunk (512 cells of one solve; chunk0 in the
+// descriptors).  Summation order depends only on the solve's own grid.
+void launch_batch_residual_norm(const BatchSolve* d, int nsolves, int total_chunks, double* part, double* l2,
+                                cudaStream_t s);
 
 // ---- full-FP64 engine (kernels_f64.cu, built with -fmad=false) ----
 // The reference-shaped engine in double on its own buffers; vertices are the solver's

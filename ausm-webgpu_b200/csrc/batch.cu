@@ -45,6 +45,7 @@ struct ausm_batch {
   cudaEvent_t fork = nullptr, join[2] = {nullptr, nullptr};
   bool uploaded = false;
   int total_tiles = 0;
+  int total_chunks = 0;  // residual-norm chunks of all members
   BatchSolve* d_solves = nullptr;
   CUtensorMap* d_maps = nullptr;  // 8 per descriptor (halo[3], plain[3], mi, mj) when tma
   bool tma = false;               // every member has tensor maps: stages load tiles by TMA
@@ -67,6 +68,7 @@ struct ausm_batch {
 namespace {
 
 constexpr int kTX = 32;  // tile width of the batched stage kernels (height: ausm_batch::rows)
+constexpr int kNormChunk = 512;  // cells per residual-norm chunk (kernels_batch.cu)
 
 int bfail(ausm_batch* b, int code, const std::string& msg) {
   ausm::set_thread_error(msg);
@@ -97,8 +99,9 @@ void drop_graphs(ausm_batch* b) {
   b->graph.clear();
 }
 
-BatchSolve describe(const ausm_solver* h, int tile0, const CUtensorMap* maps) {
+BatchSolve describe(const ausm_solver* h, int tile0, int chunk0, const CUtensorMap* maps) {
   BatchSolve d{};
+  d.chunk0 = chunk0;
   d.maps = maps;
   for (int k = 0; k < 3; k++) d.Q[k] = h->Q[k];
   d.Mi = h->Mi;
@@ -141,8 +144,8 @@ int ensure_capacity(ausm_batch* b) {
     b->cap = cap;
     b->uploaded = false;
   }
-  if (b->total_tiles > b->part_cap) {
-    int cap = std::max(b->total_tiles, 2 * b->part_cap);
+  if (b->total_chunks > b->part_cap) {
+    int cap = std::max(b->total_chunks, 2 * b->part_cap);
     BCU(b, cudaStreamSynchronize(b->st));
     cudaFree(b->d_part);
     b->d_part = nullptr;
@@ -171,16 +174,19 @@ void relayout(ausm_batch* b) {
   for (ausm_solver* h : b->members) b->tma = b->tma && h->tma[0].ok && h->tma[1].ok && h->tma[2].ok;
   if (!b->tma) b->rows = 16;
   const int rows = b->rows;
+  int chunks = 0;
   for (int k : b->order) {
     const ausm_solver* h = b->members[k];
     const int s = (int)b->mirror.size();
     if (b->groups.empty() || b->groups.back().scheme != h->p.scheme) b->groups.push_back({h->p.scheme, s, s, t, t});
-    b->mirror.push_back(describe(h, t, maps_of(b, s)));
+    b->mirror.push_back(describe(h, t, chunks, maps_of(b, s)));
     t += ((h->M + kTX - 1) / kTX) * ((h->N + rows - 1) / rows);
+    chunks += (int)(((size_t)h->M * h->N + kNormChunk - 1) / kNormChunk);
     b->groups.back().s_hi = s + 1;
     b->groups.back().t_hi = t;
   }
   b->total_tiles = t;
+  b->total_chunks = chunks;
   b->uploaded = false;
 }
 
@@ -193,7 +199,7 @@ int sync_descriptors(ausm_batch* b) {
     }
   bool changed = !b->uploaded;
   for (size_t k = 0; k < b->members.size(); k++) {
-    BatchSolve d = describe(b->members[b->order[k]], b->mirror[k].tile0, maps_of(b, (int)k));
+    BatchSolve d = describe(b->members[b->order[k]], b->mirror[k].tile0, b->mirror[k].chunk0, maps_of(b, (int)k));
     if (std::memcmp(&d, &b->mirror[k], sizeof d) != 0) {
       b->mirror[k] = d;
       changed = true;
@@ -502,7 +508,7 @@ int ausm_batch_residual_l2(ausm_batch* b, double* l2) {
   for (const ausm_batch::Group& q : b->groups)
     ausm::launch_batch_stage(q.scheme, 0, false, b->d_solves, q.s_lo, q.s_hi, q.t_lo, q.t_hi, 0, b->rows, nullptr,
                              b->st);
-  ausm::launch_batch_residual_norm(b->d_solves, ns, b->total_tiles, b->rows, b->d_part, b->d_l2, b->st);
+  ausm::launch_batch_residual_norm(b->d_solves, ns, b->total_chunks, b->d_part, b->d_l2, b->st);
   BCU(b, cudaGetLastError());
   BCU(b, cudaMemcpyAsync(b->h_l2, b->d_l2, ns * sizeof(double), cudaMemcpyDeviceToHost, b->st));
   BCU(b, cudaStreamSynchronize(b->st));

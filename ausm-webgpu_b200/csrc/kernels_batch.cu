@@ -119,24 +119,31 @@ __global__ void k_batch_gather(const BatchSolve* __restrict__ solves, int n, flo
   out[2 * s + 1] = __uint_as_float(solves[s].wave[0]);
 }
 
-// One CTA per tile: sum of (d rho / dt)^2 over the tile's cells of the stage-0 output,
-// in a fixed order (strided per-thread sums, then a shared-memory tree).
-template <int TY>
-__global__ void __launch_bounds__(256) k_batch_tile_sumsq(const BatchSolve* __restrict__ solves, int nsolves,
-                                                          double* __restrict__ part) {
-  const int item = blockIdx.x;
-  const BatchSolve& d = solves[solve_of(solves, 0, nsolves, item)];
-  const int local = item - d.tile0;
-  const int i0 = (local % d.tiles_x) * TX, j0 = (local / d.tiles_x) * TY;
+// Residual norms in a fixed order that depends only on each solve's own size: one CTA
+// per chunk of kNormChunk consecutive cells (row-major) of one solve, strided per-thread
+// sums and a shared-memory tree into part[chunk]; then one warp per solve adds its
+// chunks' partial sums (lane-strided, then a fixed butterfly).  The tile height of the
+// batch does not enter, so a solve's norm is the same in any batch.
+constexpr int kNormChunk = 512;
+
+__global__ void __launch_bounds__(256) k_batch_chunk_sumsq(const BatchSolve* __restrict__ solves, int nsolves,
+                                                           double* __restrict__ part) {
+  const int chunk = blockIdx.x;
+  int lo = 0, hi = nsolves - 1;  // the last solve whose first chunk is <= chunk
+  while (lo < hi) {
+    int mid = (lo + hi + 1) >> 1;
+    if (solves[mid].chunk0 <= chunk) lo = mid;
+    else hi = mid - 1;
+  }
+  const BatchSolve& d = solves[lo];
   const float4* R = d.Q[(d.cur + 1) % 3];
+  const size_t n = (size_t)d.M * d.N, k0 = (size_t)(chunk - d.chunk0) * kNormChunk;
   double acc = 0.0;
-  for (int k = threadIdx.x; k < TX * TY; k += 256) {
-    int i = i0 + (k % TX), j = j0 + k / TX;
-    if (i < d.M && j < d.N) {
-      double r = R[(size_t)j * d.M + i].x;
+  for (int k = threadIdx.x; k < kNormChunk; k += 256)
+    if (k0 + k < n) {
+      double r = R[k0 + k].x;
       acc += r * r;
     }
-  }
   __shared__ double sh[256];
   sh[threadIdx.x] = acc;
   __syncthreads();
@@ -144,32 +151,30 @@ __global__ void __launch_bounds__(256) k_batch_tile_sumsq(const BatchSolve* __re
     if ((int)threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
     __syncthreads();
   }
-  if (threadIdx.x == 0) part[item] = sh[0];
+  if (threadIdx.x == 0) part[chunk] = sh[0];
 }
 
-// One warp per solve: lane-strided sums over the solve's tiles, then a fixed butterfly.
-__global__ void k_batch_norm(const BatchSolve* __restrict__ solves, int nsolves, int rows,
-                             const double* __restrict__ part, double* __restrict__ l2) {
+__global__ void k_batch_norm(const BatchSolve* __restrict__ solves, int nsolves, const double* __restrict__ part,
+                             double* __restrict__ l2) {
   const int s = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
   if (s >= nsolves) return;
   const BatchSolve& d = solves[s];
-  const int ntiles = d.tiles_x * ((d.N + rows - 1) / rows);
+  const size_t n = (size_t)d.M * d.N;
+  const int nchunks = (int)((n + kNormChunk - 1) / kNormChunk);
   double acc = 0.0;
-  for (int t = lane; t < ntiles; t += 32) acc += part[d.tile0 + t];
+  for (int t = lane; t < nchunks; t += 32) acc += part[d.chunk0 + t];
   for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-  if (lane == 0) l2[s] = sqrt(acc / ((double)d.M * d.N));
+  if (lane == 0) l2[s] = sqrt(acc / (double)n);
 }
 
 void launch_batch_gather(const BatchSolve* d, int nsolves, float* out, cudaStream_t s) {
   k_batch_gather<<<(nsolves + 127) / 128, 128, 0, s>>>(d, nsolves, out);
 }
-void launch_batch_residual_norm(const BatchSolve* d, int nsolves, int total_tiles, int rows, double* part,
-                                double* l2, cudaStream_t s) {
-  if (total_tiles <= 0) return;
-  if (rows == 8) k_batch_tile_sumsq<8><<<total_tiles, 256, 0, s>>>(d, nsolves, part);
-  else if (rows == 32) k_batch_tile_sumsq<32><<<total_tiles, 256, 0, s>>>(d, nsolves, part);
-  else k_batch_tile_sumsq<16><<<total_tiles, 256, 0, s>>>(d, nsolves, part);
-  k_batch_norm<<<(nsolves + 3) / 4, 128, 0, s>>>(d, nsolves, rows, part, l2);
+void launch_batch_residual_norm(const BatchSolve* d, int nsolves, int total_chunks, double* part, double* l2,
+                                cudaStream_t s) {
+  if (total_chunks <= 0) return;
+  k_batch_chunk_sumsq<<<total_chunks, 256, 0, s>>>(d, nsolves, part);
+  k_batch_norm<<<(nsolves + 3) / 4, 128, 0, s>>>(d, nsolves, part, l2);
 }
 
 void launch_batch_dt(BatchSolve* d, int nsolves, cudaStream_t s) {

@@ -1,7 +1,7 @@
 // TMA staging of one stage tile (one tile per CTA): the state box with its 2-cell halo
 // (36 x (TY+4) float4), the face-record boxes (33 x TY i-faces, 32 x (TY+1) j-faces)
 // and, for stages 2 and 3, the Qn box (32 x TY) land in shared memory by four
-// cp.async.bulk.tensor copies (no multicast) completing on one mbarrier; the threads
+// cp.async.bulk.tensor copies (no multicast) completing on three mbarriers; the threads
 // then fill the seam columns and ghost rows the boxes cannot hold and run the tile
 // compute of stage_tile.cuh.  Used by the single-solve kernel (tensor maps as a kernel
 // parameter) and the batched kernel (per-solve tensor maps in global memory, written
@@ -24,36 +24,47 @@ template <int TY> struct T1 {
   static constexpr int SN = TY * TX * 16;              // Qn box
   static constexpr int OFF_I = r128(SQ), OFF_J = OFF_I + r128(SI), OFF_N = OFF_J + r128(SJ);
   static constexpr int OFF_BAR = OFF_N + r128(SN);
-  static constexpr int SMEM = OFF_BAR + 128 + 128;  // + alignment slack of the base
+  static constexpr int SMEM = OFF_BAR + 128 + 128;  // 3 mbarriers + alignment slack of the base
 };
 
-// Loads the tile's boxes and waits for them (thread 0 issues and polls, bounded; the
-// other threads wait at the CTA barrier).  Returns false on a timeout, after setting *err and giving the copies a second bounded wait.
+// Issues the tile's boxes (thread 0): the state box on barrier 0, the two face-record
+// boxes on barrier 1, Qn (stages 2, 3) on barrier 2, so each phase waits only for what
+// it reads.
 template <int STAGE, int TY>
-__device__ __forceinline__ bool tile_tma_load(const CUtensorMap* qs, const CUtensorMap* qn, const CUtensorMap* mi,
-                                              const CUtensorMap* mj, unsigned char* smem, int i0, int j0, int tid,
-                                              int* err) {
+__device__ __forceinline__ void tile_tma_issue(const CUtensorMap* qs, const CUtensorMap* qn, const CUtensorMap* mi,
+                                               const CUtensorMap* mj, unsigned char* smem, int i0, int j0) {
   using L = T1<TY>;
   uint64_t* bar = reinterpret_cast<uint64_t*>(smem + L::OFF_BAR);
-  if (tid == 0) {
-    mbar_init(bar, 1);
-    mbar_fence_init();
-    mbar_expect_tx(bar, L::SQ + L::SI + L::SJ + (STAGE >= 2 ? L::SN : 0));
-    tma_load_2d(smem, qs, 4 * (i0 - 2), j0 - 2, bar);
-    tma_load_2d(smem + L::OFF_I, mi, 4 * i0, j0, bar);
-    tma_load_2d(smem + L::OFF_J, mj, 4 * i0, j0, bar);
-    if (STAGE >= 2) tma_load_2d(smem + L::OFF_N, qn, 4 * i0, j0, bar);
+  mbar_init(&bar[0], 1);
+  mbar_init(&bar[1], 1);
+  mbar_init(&bar[2], 1);
+  mbar_fence_init();
+  mbar_expect_tx(&bar[0], L::SQ);
+  tma_load_2d(smem, qs, 4 * (i0 - 2), j0 - 2, &bar[0]);
+  mbar_expect_tx(&bar[1], L::SI + L::SJ);
+  tma_load_2d(smem + L::OFF_I, mi, 4 * i0, j0, &bar[1]);
+  tma_load_2d(smem + L::OFF_J, mj, 4 * i0, j0, &bar[1]);
+  if constexpr (STAGE >= 2) {
+    mbar_expect_tx(&bar[2], L::SN);
+    tma_load_2d(smem + L::OFF_N, qn, 4 * i0, j0, &bar[2]);
   }
-  // Thread 0 alone polls the barrier (bounded); the other threads wait at the CTA
-  // barrier, which issues no instructions while the boxes land, so the other CTAs on
-  // the SM keep the issue slots.  The mbarrier wait acquires the async-proxy writes
-  // for thread 0 and the CTA barrier passes them on to the rest.
+}
+
+// Thread 0 polls barrier q (bounded); the other threads wait at the CTA barrier, which
+// issues no instructions while the box lands, so co-resident CTAs keep the issue
+// slots.  The mbarrier wait acquires the async-proxy writes for thread 0 and the CTA
+// barrier passes them on to the rest.  Returns false for every thread on a timeout,
+// after thread 0 has set *err and given the copies still in flight a second bounded
+// wait.  Every thread of the CTA calls it.
+template <int STAGE, int TY>
+__device__ __forceinline__ bool tile_tma_wait(unsigned char* smem, int q, int tid, int* err) {
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem + T1<TY>::OFF_BAR);
   bool ok = true;
-  if (tid == 0) ok = mbar_wait(bar, 0);
+  if (tid == 0) ok = mbar_wait(&bar[q], 0);
   if (__syncthreads_or(!ok)) {
     if (tid == 0) {
       atomicExch(err, 1);
-      mbar_wait(bar, 0);  // let copies still in flight land before the CTA exits
+      for (int k = q; k < (STAGE >= 2 ? 3 : 2); k++) mbar_wait(&bar[k], 0);
     }
     return false;
   }
@@ -61,7 +72,7 @@ __device__ __forceinline__ bool tile_tma_load(const CUtensorMap* qs, const CUten
 }
 
 // The whole stage of tile (i0, j0); wmax gets the tile's max wave-speed bits (EMIT).
-// Returns false (nothing written) when the tile's loads timed out.
+// Returns false (nothing written) when one of the tile's loads timed out.
 template <int SCHEME, int STAGE, bool EMIT, int TY>
 __device__ __forceinline__ bool tile_tma_body(unsigned char* smem, const CUtensorMap* qs, const CUtensorMap* qn,
                                               const CUtensorMap* mi, const CUtensorMap* mj,
@@ -76,10 +87,11 @@ __device__ __forceinline__ bool tile_tma_body(unsigned char* smem, const CUtenso
   float4(*Tj)[TX] = reinterpret_cast<float4(*)[TX]>(smem + L::OFF_J);
   float4(*SN)[TX] = reinterpret_cast<float4(*)[TX]>(smem + L::OFF_N);
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * NWX + tx;
-  if (!tile_tma_load<STAGE, TY>(qs, qn, mi, mj, smem, i0, j0, tid, err)) return false;
+  if (tid == 0) tile_tma_issue<STAGE, TY>(qs, qn, mi, mj, smem, i0, j0);
+  if (!tile_tma_wait<STAGE, TY>(smem, 0, tid, err)) return false;
 
-  // fill seam columns and ghost rows the box could not hold, keep the owned conserved
-  // states, convert to primitives in place
+  // fill seam columns and ghost rows the state box could not hold, keep the owned
+  // conserved states, convert to primitives in place (the face records are landing)
   auto stage_entry = [&](int pr, int pc) {
     const int ig = i0 - 2 + pc, j = j0 - 2 + pr;
     float4 q;
@@ -99,14 +111,20 @@ __device__ __forceinline__ bool tile_tma_body(unsigned char* smem, const CUtenso
       stage_entry(hr, hc);
     }
   }
-  if (i0 + TX >= M && tx == 0) {  // the face column past the seam (zero-filled by the box)
-    for (int r = ty; r < TY; r += NWY)
-      if (j0 + r < N) Ti[r][M - i0] = __ldg(&Mi[(size_t)(j0 + r) * M]);
+  if (!tile_tma_wait<STAGE, TY>(smem, 1, tid, err)) return false;  // also orders the P writes
+  if (i0 + TX >= M) {  // uniform per CTA: the face column past the seam (zero-filled by the box)
+    if (tx == 0)
+      for (int r = ty; r < TY; r += NWY)
+        if (j0 + r < N) Ti[r][M - i0] = __ldg(&Mi[(size_t)(j0 + r) * M]);
+    __syncthreads();
   }
-  __syncthreads();
   const FaceW w = own_weights<TY>(Ti, Tj, tx, ty);
   faces_phase<SCHEME, TY>(P, Ti, Tj, c, i0, j0, M, N, tx, ty);
-  __syncthreads();
+  if constexpr (STAGE >= 2) {
+    if (!tile_tma_wait<STAGE, TY>(smem, 2, tid, err)) return false;  // also orders the flux writes
+  } else {
+    __syncthreads();
+  }
   auto qnf = [&](int h) { return SN[ty + NWY * h][tx]; };
   wmax = combine_phase<STAGE, EMIT, TY>(Ti, Tj, w, qa, qb, qnf, Qo, dt, c, i0, j0, M, N, tx, ty);
   return true;

@@ -201,8 +201,9 @@ def test_batch_errors(grids):
 
 
 def test_batch_tile_heights_bit_identical(grids, monkeypatch):
-    """The batch laid out with 8-, 16- and 32-row tiles gives the same state bits (the
-    residual norm sums per tile, so its rounding follows the tiling)."""
+    """The batch laid out with 8-, 16- and 32-row tiles gives the same state bits, and the
+    same residual norms (they are summed over fixed chunks of each solve's cells, not
+    over the batch's tiles)."""
     from ausm import Batch
     out = {}
     for rows in ("8", "16", "32"):
@@ -220,4 +221,4 @@ def test_batch_tile_heights_bit_identical(grids, monkeypatch):
     for rows in ("8", "32"):
         for a, c in zip(out[rows][0], out["16"][0]):
             np.testing.assert_array_equal(a, c)
-        np.testing.assert_allclose(out[rows][1], out["16"][1], rtol=1e-12)
+        np.testing.assert_array_equal(out[rows][1], out["16"][1])
