@@ -2,10 +2,12 @@
 
     python ausm-webgpu_b200/build.py [--force] [--verbose]
 
-Each .cu file under csrc/ is compiled by nvcc for sm_100a only; the reference-shaped
-engine and the grid/force/layout kernels are compiled with -fmad=false (no fused
-multiply-add contraction) so their float arithmetic is the reference's, operation by
-operation.  The CUDA runtime is linked statically so the library has no torch or
+Each .cu file under csrc/ is compiled by nvcc for sm_100a only, and with -fmad=false:
+the compiler contracts no multiply and add on its own.  The reference-shaped engine
+and the grid/force/layout kernels thereby keep the reference's float arithmetic
+operation by operation; the fused engines write each fused multiply-add explicitly
+(fmaf, packed f32x2), so every expression rounds the same way in every kernel that
+inlines it.  The CUDA runtime is linked statically so the library has no torch or
 Python dependency.  ptxas resource usage (-Xptxas -v) goes to lib/ptxas.log.
 """
 from __future__ import annotations
@@ -25,8 +27,7 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-I", str(ROOT / "include"), "-I", str(CSRC),
-          "-Xptxas", "-v", "--expt-relaxed-constexpr"]
-NO_FMAD = {"kernels_reference.cu", "kernels_misc.cu", "kernels_f64.cu"}
+          "-Xptxas", "-v", "--expt-relaxed-constexpr", "-fmad=false"]
 EXTRA = os.environ.get("AUSM_NVCC_EXTRA", "").split()  # tuning sweeps, e.g. -DAUSM_FUSED_MIN_BLOCKS=4
 
 
@@ -54,7 +55,7 @@ def build(force: bool = False, verbose: bool = False) -> Path:
 
     def compile_one(src: Path):
         obj = objdir / (src.stem + ".o")
-        flags = list(COMMON) + EXTRA + (["-fmad=false"] if src.name in NO_FMAD else [])
+        flags = list(COMMON) + EXTRA
         cmd = [NVCC, *ARCH, *flags, "-c", str(src), "-o", str(obj)]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:

@@ -43,7 +43,8 @@ void make_consts(ausm_solver* h) {
   c.gammaInP = g * inP;
   c.aStarK = (2.0f * c.gm1) / (g + 1.0f);
   c.ambE = inP / (g - 1.0f);
-  c.gmgm1 = g / c.gm1;
+  c.h2k = (2.0f * g) / c.gm1;
+  c.ask4 = 0.25f * c.aStarK;
   c.minfk = c.Vinf2 / c.gammaInP;
   c.muscl = p.muscl;
   h->c = c;

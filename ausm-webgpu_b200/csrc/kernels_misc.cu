@@ -150,9 +150,10 @@ __global__ void k_f2d(const float2* __restrict__ a, double2* __restrict__ b, siz
 
 // Face records in FP64, rounded once to FP32 (shaders/grid.js:115-147 computes them in
 // FP32 from FP32 vertices).  Mi[j][i]: face between cells (i-1, j) and (i, j), tangent
-// V(i, j+1) - V(i, j), unit normal (-t.y, t.x), its length, and 1 / area of cell
-// (i, j).  Mj[j][i], j = 0..N: face between cells (i, j-1) and (i, j), tangent
-// V(i, j) - V(i+1, j), normal, length, and for j < N the wave-speed factor
+// V(i, j+1) - V(i, j), unit normal (-t.y, t.x), half its length (the fused flux takes
+// twice the mass flux and pressure), and 1 / area of cell (i, j).  Mj[j][i],
+// j = 0..N: face between cells (i, j-1) and (i, j), tangent V(i, j) - V(i+1, j),
+// normal, half length, and for j < N the wave-speed factor
 // (l_l + l_r + l_u + l_d) / (2 A) of cell (i, j) (ausm.js:617-630).
 __global__ void k_metrics_d(const double2* __restrict__ V, float4* __restrict__ Mi, float4* __restrict__ Mj, int M,
                             int N) {
@@ -171,9 +172,9 @@ __global__ void k_metrics_d(const double2* __restrict__ V, float4* __restrict__ 
     double lu = sqrt((c.x - d.x) * (c.x - d.x) + (c.y - d.y) * (c.y - d.y));
     double A = 0.5 * fabs((d.x - a.x) * (c.y - b.y) - (c.x - b.x) * (d.y - a.y));
     w = (float)((ll + lr + lu + ld) / (2.0 * A));
-    Mi[(size_t)j * M + i] = make_float4((float)(-uy / ll), (float)(ux / ll), (float)ll, (float)(1.0 / A));
+    Mi[(size_t)j * M + i] = make_float4((float)(-uy / ll), (float)(ux / ll), (float)(0.5 * ll), (float)(1.0 / A));
   }
-  Mj[(size_t)j * M + i] = make_float4((float)(-ty / ld), (float)(tx / ld), (float)ld, w);
+  Mj[(size_t)j * M + i] = make_float4((float)(-ty / ld), (float)(tx / ld), (float)(0.5 * ld), w);
 }
 
 // ---- surface force (graphs.js:186-272): FP32 pressure of the first interior cell,

@@ -63,7 +63,7 @@ __global__ void k_ref_flux_j(const float4* __restrict__ st, const float2* __rest
   float nx, ny, len;
   edge_normal<false>(V[(size_t)j * M + i], V[(size_t)j * M + (i + 1) % M], nx, ny, len);
   const float gm1 = c.gm1;
-  float4 f = face_flux<SCHEME, false>(to_prim<false>(ref_load(st, M, i, j - 2), gm1),
+  float4 f = face_flux<SCHEME>(to_prim<false>(ref_load(st, M, i, j - 2), gm1),
                                       to_prim<false>(ref_load(st, M, i, j - 1), gm1),
                                       to_prim<false>(ref_load(st, M, i, j), gm1),
                                       to_prim<false>(ref_load(st, M, i, j + 1), gm1), nx, ny, c);
@@ -78,7 +78,7 @@ __global__ void k_ref_flux_i(const float4* __restrict__ st, const float2* __rest
   float nx, ny, len;
   edge_normal<false>(V[(size_t)(j + 1) * M + i], V[(size_t)j * M + i], nx, ny, len);
   const float gm1 = c.gm1;
-  float4 f = face_flux<SCHEME, false>(to_prim<false>(ref_load(st, M, i - 2, j), gm1),
+  float4 f = face_flux<SCHEME>(to_prim<false>(ref_load(st, M, i - 2, j), gm1),
                                       to_prim<false>(ref_load(st, M, i - 1, j), gm1),
                                       to_prim<false>(ref_load(st, M, i, j), gm1),
                                       to_prim<false>(ref_load(st, M, i + 1, j), gm1), nx, ny, c);

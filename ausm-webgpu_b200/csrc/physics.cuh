@@ -1,13 +1,19 @@
 // Device arithmetic of the AUSM-family solver: primitive conversion, ghost cells,
 // MUSCL/van Albada interface states and the SLAU2 / SLAU / AUSM+-up fluxes.
 //
-// Every function takes a template flag FAST.  FAST=false spells each operation as
-// the reference writes it (IEEE division and square root, same operation order); the
-// reference-shaped engine is compiled with -fmad=false so it reproduces the CPU oracle
-// bit for bit.  FAST=true is the fused engine's arithmetic: approximate reciprocal
-// and square root (one MUFU instruction each, about 1 ulp), shared reciprocals and an
-// algebraically equal van Albada form; its parity bound against the oracle is tested
-// at 1e-5.
+// Functions with a template flag FAST: FAST=false spells each operation as the
+// reference writes it (IEEE division and square root, same operation order), and
+// face_flux / muscl1 are that form only; the reference-shaped engine reproduces the CPU
+// oracle bit for bit with them.  FAST=true, muscl2_packed and face_flux_len are the
+// fused engines' arithmetic: approximate reciprocal and square root (one MUFU
+// instruction each, about 1 ulp), shared reciprocals, an algebraically equal van
+// Albada form and every fused multiply-add written out (fmaf / packed f32x2); its
+// parity bound against the oracle is tested at 1e-5.
+//
+// Every translation unit that includes this file is compiled with -fmad=false, so the
+// compiler contracts nothing on its own: the rounding of each expression is fixed by
+// its source, not by the code around an inlined copy, and two kernels that compute the
+// same face or cell (for instance tiles of different heights) give the same bits.
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -26,7 +32,8 @@ struct Consts {
   float gammaInP;  // gamma*inP                           ausm.js:273
   float aStarK;    // (2*gm1)/(gamma+1)                   ausm.js:278
   float ambE;      // inP/(gamma-1)                       ausm.js:108
-  float gmgm1;     // gamma/(gamma-1), fast enthalpy form (FAST only)
+  float h2k;       // 2 gamma/(gamma-1): twice the total enthalpy is h2k p/rho + |v|^2 (FAST only)
+  float ask4;      // aStarK/4: the AUSM+-up a*^2 from twice the enthalpies (FAST only)
   float minfk;     // Vinf2/gammaInP: the AUSM+-up M_inf^2 from rho_L is rho_L * minfk (FAST only)
   int muscl;
 };
@@ -86,15 +93,18 @@ __device__ __forceinline__ void edge_normal(float2 a, float2 b, float& nx, float
 
 // toPrimitive (ausm.js:145-150): (rho, u, v, p), p >= 1e-7
 template <bool FAST> __device__ __forceinline__ float4 to_prim(float4 Q, float gm1) {
-  float rho = Q.x, u, v;
+  float rho = Q.x;
   if constexpr (FAST) {
-    float ir = frcp<true>(rho);
-    u = Q.y * ir; v = Q.z * ir;
+    // rho |v|^2 as (rho u) u + (rho v) v
+    const float ir = frcp<true>(rho);
+    const float u = Q.y * ir, v = Q.z * ir;
+    const float k = fmaf(Q.z, v, Q.y * u);
+    return make_float4(rho, u, v, fmaxf(1e-7f, fmaf(-0.5f, k, Q.w) * gm1));
   } else {
-    u = Q.y / rho; v = Q.z / rho;
+    float u = Q.y / rho, v = Q.z / rho;
+    float p = fmaxf(1e-7f, (Q.w - 0.5f * rho * (u * u + v * v)) * gm1);
+    return make_float4(rho, u, v, p);
   }
-  float p = fmaxf(1e-7f, (Q.w - 0.5f * rho * (u * u + v * v)) * gm1);
-  return make_float4(rho, u, v, p);
 }
 
 // Wall ghost (ausm.js:57-64): velocity of the first interior cell reflected about the
@@ -160,98 +170,72 @@ __device__ __forceinline__ void far_ghosts(float4 s, float2 a, float2 b, const C
 }
 
 // van Albada-limited MUSCL on two primitive components at once (packed f32x2), the
-// FAST form of muscl1: phi(r) = n (n + d) / (n^2 + d^2), r = n / d.
+// FAST form of muscl1: phi(r) = n (n + d) / (n^2 + d^2) with r = n / d, one reciprocal
+// per side and none for r itself.  The right side takes the reciprocal of -q (the
+// same magnitude), so both sides add phi x dF/2 with one shared dF/2.
 __device__ __forceinline__ void muscl2_packed(float2 l2, float2 l, float2 r, float2 r2, float2& lo, float2& ro) {
   const float2 eps = make_float2(1e-6f, 1e-6f), m1 = make_float2(-1.0f, -1.0f);
-  const float2 half = make_float2(0.5f, 0.5f), mhalf = make_float2(-0.5f, -0.5f);
+  const float2 half = make_float2(0.5f, 0.5f);
   // differences as x*(-1) + y: exact products, one rounding, no separate negation
-  float2 dL = fma2(l2, m1, l), dF = fma2(l, m1, r), dR = fma2(r, m1, r2);
-  float2 den = fma2(dF, dF, eps);
-  float2 nL = fma2(dL, dF, eps), nR = fma2(dF, dR, eps);
-  float2 d2 = mul2(den, den);
-  float2 qL = fma2(nL, nL, d2), qR = fma2(nR, nR, d2);
-  float2 rqL = make_float2(rcp_approx(qL.x), rcp_approx(qL.y));
-  float2 rqR = make_float2(rcp_approx(qR.x), rcp_approx(qR.y));
-  float2 tL = mul2(nL, add2(nL, den)), tR = mul2(nR, add2(nR, den));
-  lo = fma2(mul2(tL, rqL), mul2(half, dF), l);
-  ro = fma2(mul2(tR, rqR), mul2(mhalf, dF), r);
+  const float2 dL = fma2(l2, m1, l), dF = fma2(l, m1, r), dR = fma2(r, m1, r2);
+  const float2 den = fma2(dF, dF, eps);
+  const float2 nL = fma2(dL, dF, eps), nR = fma2(dF, dR, eps);
+  const float2 d2 = mul2(den, den);
+  const float2 qL = fma2(nL, nL, d2), qR = fma2(nR, nR, d2);
+  const float2 rqL = make_float2(rcp_approx(qL.x), rcp_approx(qL.y));
+  const float2 rqR = make_float2(rcp_approx(-qR.x), rcp_approx(-qR.y));
+  const float2 tL = mul2(nL, add2(nL, den)), tR = mul2(nR, add2(nR, den));
+  const float2 hdF = mul2(half, dF);
+  lo = fma2(mul2(tL, rqL), hdF, l);
+  ro = fma2(mul2(tR, rqR), hdF, r);
 }
 
 // van Albada-limited MUSCL update of one primitive component (ausm.js:238-249).
-template <bool FAST>
 __device__ __forceinline__ void muscl1(float l2, float l, float r, float r2, float& lo, float& ro) {
   const float eps = 1e-6f;
   float dL = l - l2, dF = r - l, dR = r2 - r;
   float den = dF * dF + eps;
   float nL = dL * dF + eps, nR = dF * dR + eps;
-  if constexpr (FAST) {
-    // phi(n/d) = (r^2 + r)/(r^2 + 1) = n (n + d) / (n^2 + d^2) with r = n/d: one
-    // reciprocal per side and no division for r itself.
-    float d2 = den * den;
-    float qL = nL * nL + d2, qR = nR * nR + d2;
-    float phiL = nL * (nL + den) * frcp<true>(qL);
-    float phiR = nR * (nR + den) * frcp<true>(qR);
-    lo = l + 0.5f * phiL * dF;
-    ro = r - 0.5f * phiR * dF;
-  } else {
-    float rL = nL / den, rR = nR / den;
-    float r2L = rL * rL, r2R = rR * rR;
-    lo = l + 0.5f * ((r2L + rL) / (r2L + 1.0f)) * dF;
-    ro = r - 0.5f * ((r2R + rR) / (r2R + 1.0f)) * dF;
-  }
+  float rL = nL / den, rR = nR / den;
+  float r2L = rL * rL, r2R = rR * rR;
+  lo = l + 0.5f * ((r2L + rL) / (r2L + 1.0f)) * dF;
+  ro = r - 0.5f * ((r2R + rR) / (r2R + 1.0f)) * dF;
 }
 
 // Flux per unit face length through a face with unit normal (nx, ny) pointing from
 // L to R, from the primitive states of the four cells along the face normal line
 // (fluxInterfaceStateCode ausm.js:201-266 + SLAUFluxShaderCode ausm.js:348-391 /
 // AUSMupFluxShaderCode ausm.js:273-334).
-template <int SCHEME, bool FAST>
+template <int SCHEME>
 __device__ __forceinline__ float4 face_flux(float4 L2, float4 L, float4 R, float4 R2, float nx, float ny,
                                             const Consts& c) {
   float4 Lm = L, Rm = R;
   if (c.muscl > 0) {
-    if constexpr (FAST) {
-      float2 a, b;
-      muscl2_packed(lo2(L2), lo2(L), lo2(R), lo2(R2), a, b);
-      Lm.x = a.x; Lm.y = a.y; Rm.x = b.x; Rm.y = b.y;
-      muscl2_packed(hi2(L2), hi2(L), hi2(R), hi2(R2), a, b);
-      Lm.z = a.x; Lm.w = a.y; Rm.z = b.x; Rm.w = b.y;
-    } else {
-      muscl1<FAST>(L2.x, L.x, R.x, R2.x, Lm.x, Rm.x);
-      muscl1<FAST>(L2.y, L.y, R.y, R2.y, Lm.y, Rm.y);
-      muscl1<FAST>(L2.z, L.z, R.z, R2.z, Lm.z, Rm.z);
-      muscl1<FAST>(L2.w, L.w, R.w, R2.w, Lm.w, Rm.w);
-    }
+    muscl1(L2.x, L.x, R.x, R2.x, Lm.x, Rm.x);
+    muscl1(L2.y, L.y, R.y, R2.y, Lm.y, Rm.y);
+    muscl1(L2.z, L.z, R.z, R2.z, Lm.z, Rm.z);
+    muscl1(L2.w, L.w, R.w, R2.w, Lm.w, Rm.w);
   }
   const float gm1 = c.gm1;
   float rhoL = Lm.x, rhoR = Rm.x, pL = Lm.w, pR = Rm.w;
   float vxL = Lm.y, vyL = Lm.z, vxR = Rm.y, vyR = Rm.z;
   float uL = vxL * nx + vyL * ny, uR = vxR * nx + vyR * ny;
   float kL = vxL * vxL + vyL * vyL, kR = vxR * vxR + vyR * vyR;
-  float hL, hR, irL = 0.0f, irR = 0.0f;
-  if constexpr (FAST) {
-    irL = frcp<true>(rhoL); irR = frcp<true>(rhoR);
-    hL = c.gmgm1 * pL * irL + 0.5f * kL;
-    hR = c.gmgm1 * pR * irR + 0.5f * kR;
-  } else {
-    hL = pL / (gm1 * rhoL) + 0.5f * kL + pL / rhoL;
-    hR = pR / (gm1 * rhoR) + 0.5f * kR + pR / rhoR;
-  }
+  float hL = pL / (gm1 * rhoL) + 0.5f * kL + pL / rhoL;
+  float hR = pR / (gm1 * rhoR) + 0.5f * kR + pR / rhoR;
   float mdot, P;
   if constexpr (SCHEME == 2) {  // AUSM+-up, Liou 2006 eqs. 28-30, 69-76
-    float Minf2 = fdiv<FAST>(c.Vinf2, fdiv<FAST>(c.gammaInP, rhoL));
+    float Minf2 = c.Vinf2 / (c.gammaInP / rhoL);
     const float sigma = 1.0f;
     float ht = 0.5f * (hL + hR);
-    float aStar = fsqrt<FAST>(fmaxf(1e-6f, c.aStarK * ht));
+    float aStar = sqrtf(fmaxf(1e-6f, c.aStarK * ht));
     float as2 = aStar * aStar;
-    float aHL = fdiv<FAST>(as2, fmaxf(uL, aStar));
-    float aHR = fdiv<FAST>(as2, fmaxf(-uR, aStar));
+    float aHL = as2 / fmaxf(uL, aStar);
+    float aHR = as2 / fmaxf(-uR, aStar);
     float a = fminf(aHL, aHR);
-    float ia = frcp<FAST>(a);
-    float ML, MR;
-    if constexpr (FAST) { ML = uL * ia; MR = uR * ia; } else { ML = uL / a; MR = uR / a; }
+    float ML = uL / a, MR = uR / a;
     float a2 = a * a;
-    float Mbar2 = fdiv<FAST>(uL * uL + uR * uR, a2 * 2.0f);
+    float Mbar2 = (uL * uL + uR * uR) / (a2 * 2.0f);
     float Mo2 = fminf(1.0f, fmaxf(Mbar2, Minf2));
     float fa = Mo2 * (2.0f - Mo2);
     float rhoI = 0.5f * (rhoL + rhoR);
@@ -261,146 +245,111 @@ __device__ __forceinline__ float4 face_flux(float4 L2, float4 L, float4 R, float
     bool supL = 1.0f <= fabsf(ML), supR = 1.0f <= fabsf(MR);
     float M4L = supL ? fmaxf(0.0f, ML) : M2pL * (1.0f + 2.0f * M2mL);
     float M4R = supR ? fminf(0.0f, MR) : M2mR * (1.0f - 2.0f * M2pR);
-    float Mi = M4L + M4R - fdiv<FAST>(c.Kp / fa * fmaxf(1.0f - sigma * Mbar2, 0.0f) * (pR - pL), rhoI * a2);
+    float Mi = M4L + M4R - (c.Kp / fa * fmaxf(1.0f - sigma * Mbar2, 0.0f) * (pR - pL)) / (rhoI * a2);
     float alpha4 = 0.75f * (-4.0f + 5.0f * fa * fa);
     float P5L = supL ? (0.0f <= ML ? 1.0f : 0.0f) : M2pL * ((2.0f - ML) + alpha4 * ML * M2mL);
     float P5R = supR ? (0.0f <= -MR ? 1.0f : 0.0f) : M2mR * ((-2.0f - MR) - alpha4 * MR * M2pR);
     P = (P5L * pL + P5R * pR) - c.Ku * P5L * P5R * (rhoL + rhoR) * fa * a * (uR - uL);
     mdot = a * Mi * (Mi > 0.0f ? rhoL : rhoR);
   } else {  // SLAU2 (SCHEME 0, Kitamura-Shima 2013) / SLAU (SCHEME 1, Shima-Kitamura 2011)
-    float aL, aR;
-    if constexpr (FAST) {
-      // 1/max(rho, 1e-10) from the already computed 1/rho
-      float igL = rhoL > 1e-10f ? irL : 1e10f, igR = rhoR > 1e-10f ? irR : 1e10f;
-      aL = fsqrt<true>(c.gamma * fmaxf(pL, 1e-10f) * igL);
-      aR = fsqrt<true>(c.gamma * fmaxf(pR, 1e-10f) * igR);
-    } else {
-      aL = sqrtf(c.gamma * fmaxf(pL, 1e-10f) / fmaxf(rhoL, 1e-10f));
-      aR = sqrtf(c.gamma * fmaxf(pR, 1e-10f) / fmaxf(rhoR, 1e-10f));
-    }
+    float aL = sqrtf(c.gamma * fmaxf(pL, 1e-10f) / fmaxf(rhoL, 1e-10f));
+    float aR = sqrtf(c.gamma * fmaxf(pR, 1e-10f) / fmaxf(rhoR, 1e-10f));
     float a = (aL + aR) * 0.5f;
-    float ia = frcp<FAST>(a);
-    float ML, MR, Uarc, Marc;
-    Uarc = fsqrt<FAST>(0.5f * (kL + kR));
-    if constexpr (FAST) {
-      ML = uL * ia; MR = uR * ia;
-      Marc = fminf(1.0f, Uarc * ia);
-    } else {
-      ML = uL / a; MR = uR / a;
-      Marc = fminf(1.0f, Uarc / a);
-    }
+    float Uarc = sqrtf(0.5f * (kL + kR));
+    float ML = uL / a, MR = uR / a;
+    float Marc = fminf(1.0f, Uarc / a);
     float X = (1.0f - Marc) * (1.0f - Marc);
     float mpL = ML + 1.0f, mmR = MR - 1.0f;
     float sqL = 0.5f * mpL * mpL, sqR = 0.5f * mmR * mmR;
     bool supL = 1.0f <= fabsf(ML), supR = 1.0f <= fabsf(MR);
-    float fpp, fpm;
-    if constexpr (FAST) {
-      // supersonic branch: 0.5 (1 + sign M) is 1 or 0 (|M| >= 1, so M != 0)
-      fpp = supL ? (ML > 0.0f ? 1.0f : 0.0f) : __saturatef(0.5f * (sqL * (2.0f - ML)));
-      fpm = supR ? (MR > 0.0f ? 0.0f : 1.0f) : __saturatef(0.5f * (sqR * (2.0f + MR)));
-    } else {
-      fpp = sat(0.5f * (supL ? 1.0f + 1.0f * wsign(ML) : sqL * (2.0f - 1.0f * ML)));
-      fpm = sat(0.5f * (supR ? 1.0f + -1.0f * wsign(MR) : sqR * (2.0f - -1.0f * MR)));
-    }
+    float fpp = sat(0.5f * (supL ? 1.0f + 1.0f * wsign(ML) : sqL * (2.0f - 1.0f * ML)));
+    float fpm = sat(0.5f * (supR ? 1.0f + -1.0f * wsign(MR) : sqR * (2.0f - -1.0f * MR)));
     if constexpr (SCHEME == 0)
       P = 0.5f * ((fpp - fpm) * (pL - pR) + (pL + pR) + (Uarc * (fpp + fpm - 1.0f) * (rhoL + rhoR) * a));
     else
       P = 0.5f * ((fpp - fpm) * (pL - pR) + (1.0f + (1.0f - X) * (fpp + fpm - 1.0f)) * (pL + pR));
     float dp = pR - pL;
-    float ubar = fdiv<FAST>(rhoL * fabsf(uL) + rhoR * fabsf(uR), rhoL + rhoR);
-    float g = FAST ? __saturatef(-ML) * __saturatef(MR) : sat(-ML) * sat(MR);
+    float ubar = (rhoL * fabsf(uL) + rhoR * fabsf(uR)) / (rhoL + rhoR);
+    float g = sat(-ML) * sat(MR);
     float ubp = ubar * (1.0f - g) + fabsf(uL) * g;
     float ubm = ubar * (1.0f - g) + fabsf(uR) * g;
-    float Xa;
-    if constexpr (FAST) Xa = X * ia; else Xa = X / a;
-    mdot = 0.5f * ((rhoL * (uL + ubp) + rhoR * (uR - ubm)) * (1.0f - g) - Xa * dp);
+    mdot = 0.5f * ((rhoL * (uL + ubp) + rhoR * (uR - ubm)) * (1.0f - g) - X / a * dp);
   }
-  (void)irL; (void)irR;
   bool left = mdot > 0.0f;
   float p1 = left ? vxL : vxR, p2 = left ? vyL : vyR, p3 = left ? hL : hR;
   return make_float4(1.0f * mdot + 0.0f, p1 * mdot + nx * P, p2 * mdot + ny * P, p3 * mdot + 0.0f);
 }
 
-// FAST flux x face length (the fused engines): face_flux<SCHEME, true> with the length
-// folded into the mass flux and pressure (two multiplies instead of four), no "+ 0"
-// terms (those keep the reference's sign of zero in the exact path); for SLAU / SLAU2
-// 1/rho guarded by one max and the pressure-split functions as the cubic
-// f(M) = (M+1)^2 (2-M) / 4 of the Mach number clamped to [-1, 1], which is exactly the
-// reference's branch (|M| >= 1 gives 1 or 0, and the cubic is 1 at M = 1, 0 at M = -1,
-// within [0, 1] between, so the saturate is a no-op there).
+// FAST flux x face length (the fused engines), from the face's half length hl: the
+// arithmetic of face_flux with approximate reciprocals and square roots, every fused
+// multiply-add written out, and these algebraic rewrites:
+//  - the length folded into the mass flux and pressure; SLAU / SLAU2 compute twice
+//    the mass flux and twice the pressure and multiply them by hl (two multiplies by
+//    0.5 fewer), AUSM+-up multiplies by hl + hl;
+//  - twice the total enthalpy h2 = h2k p / rho + |v|^2, so that no 0.5 |v|^2 is
+//    formed; the energy flux is h2 x (mass flux x hl);
+//  - no "+ 0" terms (those keep the reference's sign of zero in the exact path);
+//  - SLAU / SLAU2: 1/rho guarded by one max, the pressure-split functions as the cubic
+//    f(M) = (M+1)^2 (2-M) / 4 of the Mach number clamped to [-1, 1], which is exactly
+//    the reference's branch (|M| >= 1 gives 1 or 0, the cubic is 1 at M = 1, 0 at
+//    M = -1 and within [0, 1] between, so the saturate is a no-op there);
+//  - AUSM+-up: M_inf^2 from rho_L as rho_L Vinf^2 / (gamma p_inf); a*^2 as
+//    (aStarK / 4) (h2L + h2R), used as computed (not the square of its square root);
+//    Mbar^2 = (ML^2 + MR^2) / 2 from the face Mach numbers; the K_p pressure-diffusion
+//    term only when K_p != 0 (uniform per solve; the reference's default is 0).
 template <int SCHEME>
 __device__ __forceinline__ float4 face_flux_len(float4 L2, float4 L, float4 R, float4 R2, float nx, float ny,
-                                                float len, const Consts& c) {
-  if constexpr (SCHEME == 2) {
-    // AUSM+-up (Liou 2006 eqs. 28-30, 69-76), as face_flux<2, true> with: M_inf^2 from
-    // rho_L as rho_L * Vinf^2 / (gamma p_inf) (one multiply for two divisions); the star
-    // speed squared used as computed (not the square of its square root); Mbar^2 =
-    // (ML^2 + MR^2) / 2 from the face Mach numbers; the K_p pressure-diffusion term only
-    // when K_p != 0 (uniform per solve; the reference's default is 0); the face length
-    // folded into the mass flux and pressure.
-    float4 Lm = L, Rm = R;
-    if (c.muscl > 0) {
-      float2 a, b;
-      muscl2_packed(lo2(L2), lo2(L), lo2(R), lo2(R2), a, b);
-      Lm.x = a.x; Lm.y = a.y; Rm.x = b.x; Rm.y = b.y;
-      muscl2_packed(hi2(L2), hi2(L), hi2(R), hi2(R2), a, b);
-      Lm.z = a.x; Lm.w = a.y; Rm.z = b.x; Rm.w = b.y;
-    }
-    const float rhoL = Lm.x, rhoR = Rm.x, pL = Lm.w, pR = Rm.w;
-    const float vxL = Lm.y, vyL = Lm.z, vxR = Rm.y, vyR = Rm.z;
-    const float uL = vxL * nx + vyL * ny, uR = vxR * nx + vyR * ny;
-    const float kL = vxL * vxL + vyL * vyL, kR = vxR * vxR + vyR * vyR;
+                                                float hl, const Consts& c) {
+  float4 Lm = L, Rm = R;
+  if (c.muscl > 0) {
+    float2 a, b;
+    muscl2_packed(lo2(L2), lo2(L), lo2(R), lo2(R2), a, b);
+    Lm.x = a.x; Lm.y = a.y; Rm.x = b.x; Rm.y = b.y;
+    muscl2_packed(hi2(L2), hi2(L), hi2(R), hi2(R2), a, b);
+    Lm.z = a.x; Lm.w = a.y; Rm.z = b.x; Rm.w = b.y;
+  }
+  const float rhoL = Lm.x, rhoR = Rm.x, pL = Lm.w, pR = Rm.w;
+  const float vxL = Lm.y, vyL = Lm.z, vxR = Rm.y, vyR = Rm.z;
+  const float uL = fmaf(vyL, ny, vxL * nx), uR = fmaf(vyR, ny, vxR * nx);
+  const float kL = fmaf(vyL, vyL, vxL * vxL), kR = fmaf(vyR, vyR, vxR * vxR);
+  if constexpr (SCHEME == 2) {  // AUSM+-up, Liou 2006 eqs. 28-30, 69-76
     const float irL = frcp<true>(rhoL), irR = frcp<true>(rhoR);
-    const float hL = c.gmgm1 * pL * irL + 0.5f * kL;
-    const float hR = c.gmgm1 * pR * irR + 0.5f * kR;
+    const float h2L = fmaf(c.h2k * pL, irL, kL), h2R = fmaf(c.h2k * pR, irR, kR);
     const float Minf2 = rhoL * c.minfk;
-    const float ht = 0.5f * (hL + hR);
-    const float as2 = fmaxf(1e-6f, c.aStarK * ht);
+    const float as2 = fmaxf(1e-6f, c.ask4 * (h2L + h2R));
     const float aStar = fsqrt<true>(as2);
     const float aHL = as2 * frcp<true>(fmaxf(uL, aStar));
     const float aHR = as2 * frcp<true>(fmaxf(-uR, aStar));
     const float a = fminf(aHL, aHR);
     const float ia = frcp<true>(a);
     const float ML = uL * ia, MR = uR * ia;
-    const float Mbar2 = 0.5f * (ML * ML + MR * MR);
+    const float Mbar2 = 0.5f * fmaf(MR, MR, ML * ML);
     const float Mo2 = fminf(1.0f, fmaxf(Mbar2, Minf2));
     const float fa = Mo2 * (2.0f - Mo2);
     const float Mp1L = ML + 1.0f, Mp1R = MR + 1.0f, Mm1L = ML - 1.0f, Mm1R = MR - 1.0f;
     const float M2pL = 0.25f * Mp1L * Mp1L, M2pR = 0.25f * Mp1R * Mp1R;
     const float M2mL = -0.25f * Mm1L * Mm1L, M2mR = -0.25f * Mm1R * Mm1R;
     const bool supL = 1.0f <= fabsf(ML), supR = 1.0f <= fabsf(MR);
-    const float M4L = supL ? fmaxf(0.0f, ML) : M2pL * (1.0f + 2.0f * M2mL);
-    const float M4R = supR ? fminf(0.0f, MR) : M2mR * (1.0f - 2.0f * M2pR);
+    const float M4L = supL ? fmaxf(0.0f, ML) : M2pL * fmaf(2.0f, M2mL, 1.0f);
+    const float M4R = supR ? fminf(0.0f, MR) : M2mR * fmaf(-2.0f, M2pR, 1.0f);
     float Mi = M4L + M4R;
     if (c.Kp != 0.0f) {
       const float rhoI = 0.5f * (rhoL + rhoR);
       Mi -= c.Kp * frcp<true>(fa) * fmaxf(1.0f - Mbar2, 0.0f) * (pR - pL) * frcp<true>(rhoI * a * a);
     }
-    const float alpha4 = 0.75f * (-4.0f + 5.0f * fa * fa);
-    const float P5L = supL ? (0.0f <= ML ? 1.0f : 0.0f) : M2pL * ((2.0f - ML) + alpha4 * ML * M2mL);
-    const float P5R = supR ? (0.0f <= -MR ? 1.0f : 0.0f) : M2mR * ((-2.0f - MR) - alpha4 * MR * M2pR);
-    const float P = (P5L * pL + P5R * pR) - c.Ku * P5L * P5R * (rhoL + rhoR) * fa * a * (uR - uL);
+    const float alpha4 = 0.75f * fmaf(5.0f * fa, fa, -4.0f);
+    const float P5L = supL ? (0.0f <= ML ? 1.0f : 0.0f) : M2pL * fmaf(alpha4 * ML, M2mL, 2.0f - ML);
+    const float P5R = supR ? (0.0f <= -MR ? 1.0f : 0.0f) : M2mR * fmaf(-alpha4 * MR, M2pR, -2.0f - MR);
+    const float P = fmaf(P5L, pL, P5R * pR) - c.Ku * P5L * P5R * (rhoL + rhoR) * fa * a * (uR - uL);
     const float mdot = a * Mi * (Mi > 0.0f ? rhoL : rhoR);
     const bool left = mdot > 0.0f;
-    const float ml = mdot * len, Pl = P * len;
-    const float p1 = left ? vxL : vxR, p2 = left ? vyL : vyR, p3 = left ? hL : hR;
-    return make_float4(ml, fmaf(p1, ml, nx * Pl), fmaf(p2, ml, ny * Pl), p3 * ml);
-  } else {
-    float4 Lm = L, Rm = R;
-    if (c.muscl > 0) {
-      float2 a, b;
-      muscl2_packed(lo2(L2), lo2(L), lo2(R), lo2(R2), a, b);
-      Lm.x = a.x; Lm.y = a.y; Rm.x = b.x; Rm.y = b.y;
-      muscl2_packed(hi2(L2), hi2(L), hi2(R), hi2(R2), a, b);
-      Lm.z = a.x; Lm.w = a.y; Rm.z = b.x; Rm.w = b.y;
-    }
-    const float rhoL = Lm.x, rhoR = Rm.x, pL = Lm.w, pR = Rm.w;
-    const float vxL = Lm.y, vyL = Lm.z, vxR = Rm.y, vyR = Rm.z;
-    const float uL = vxL * nx + vyL * ny, uR = vxR * nx + vyR * ny;
-    const float kL = vxL * vxL + vyL * vyL, kR = vxR * vxR + vyR * vyR;
+    const float len = hl + hl;
+    const float ml = mdot * len, Pl = P * len, mlh = mdot * hl;
+    const float p1 = left ? vxL : vxR, p2 = left ? vyL : vyR, p3 = left ? h2L : h2R;
+    return make_float4(ml, fmaf(p1, ml, nx * Pl), fmaf(p2, ml, ny * Pl), p3 * mlh);
+  } else {  // SLAU2 (SCHEME 0, Kitamura-Shima 2013) / SLAU (SCHEME 1, Shima-Kitamura 2011)
     const float irL = frcp<true>(fmaxf(rhoL, 1e-10f)), irR = frcp<true>(fmaxf(rhoR, 1e-10f));
-    const float hL = c.gmgm1 * pL * irL + 0.5f * kL;
-    const float hR = c.gmgm1 * pR * irR + 0.5f * kR;
+    const float h2L = fmaf(c.h2k * pL, irL, kL), h2R = fmaf(c.h2k * pR, irR, kR);
     const float aL = fsqrt<true>(c.gamma * fmaxf(pL, 1e-10f) * irL);
     const float aR = fsqrt<true>(c.gamma * fmaxf(pR, 1e-10f) * irR);
     const float a = (aL + aR) * 0.5f;
@@ -414,22 +363,23 @@ __device__ __forceinline__ float4 face_flux_len(float4 L2, float4 L, float4 R, f
     const float fpp = qL * qL * (2.0f - mL);  // f(ML)
     const float fpm = qR * qR * (2.0f - mR);  // f(-MR)
     const float rs = rhoL + rhoR;
-    float P;
+    const float dpLR = pL - pR, s1 = (fpp + fpm) - 1.0f;
+    float P2;  // 2 P
     if constexpr (SCHEME == 0)
-      P = 0.5f * ((fpp - fpm) * (pL - pR) + (pL + pR) + (Uarc * (fpp + fpm - 1.0f) * rs * a));
+      P2 = fmaf(Uarc * s1 * rs, a, fmaf(fpp - fpm, dpLR, pL + pR));
     else
-      P = 0.5f * ((fpp - fpm) * (pL - pR) + (1.0f + (1.0f - X) * (fpp + fpm - 1.0f)) * (pL + pR));
-    const float dp = pR - pL;
-    const float ubar = (rhoL * fabsf(uL) + rhoR * fabsf(uR)) * frcp<true>(rs);
+      P2 = fmaf(fpp - fpm, dpLR, fmaf(1.0f - X, s1, 1.0f) * (pL + pR));
+    const float ubar = fmaf(rhoL, fabsf(uL), rhoR * fabsf(uR)) * frcp<true>(rs);
     const float g = __saturatef(-ML) * __saturatef(MR);
     const float omg = 1.0f - g;
-    const float ubp = ubar * omg + fabsf(uL) * g;
-    const float ubm = ubar * omg + fabsf(uR) * g;
-    const float mdot = 0.5f * ((rhoL * (uL + ubp) + rhoR * (uR - ubm)) * omg - X * ia * dp);
-    const bool left = mdot > 0.0f;
-    const float ml = mdot * len, Pl = P * len;
-    const float p1 = left ? vxL : vxR, p2 = left ? vyL : vyR, p3 = left ? hL : hR;
-    return make_float4(ml, fmaf(p1, ml, nx * Pl), fmaf(p2, ml, ny * Pl), p3 * ml);
+    const float ubo = ubar * omg;
+    const float ubp = fmaf(fabsf(uL), g, ubo), ubm = fmaf(fabsf(uR), g, ubo);
+    // 2 mdot = (rhoL (uL + ubp) + rhoR (uR - ubm)) (1 - g) - X/a (pR - pL)
+    const float md2 = fmaf(X * ia, dpLR, fmaf(rhoL, uL + ubp, rhoR * (uR - ubm)) * omg);
+    const bool left = md2 > 0.0f;
+    const float ml = md2 * hl, Pl = P2 * hl;
+    const float p1 = left ? vxL : vxR, p2 = left ? vyL : vyR, p3 = left ? h2L : h2R;
+    return make_float4(ml, fmaf(p1, ml, nx * Pl), fmaf(p2, ml, ny * Pl), p3 * (0.5f * ml));
   }
 }
 
@@ -447,12 +397,20 @@ template <bool FAST> __device__ __forceinline__ float wave_speed(float4 s, float
 // ... with the cell's precomputed factor W = sum(l) / (2 A)
 template <bool FAST> __device__ __forceinline__ float wave_speed_w(float4 s, float W, float gamma) {
   float rho = s.x;
-  float u = fdiv<FAST>(s.y, rho), v = fdiv<FAST>(s.z, rho);
-  float p = (s.w - 0.5f * rho * (u * u + v * v)) * (gamma - 1.0f);
-  float T = fdiv<FAST>(p, rho);
-  float a = fsqrt<FAST>(gamma * T);
-  float speed = fsqrt<FAST>(u * u + v * v);
-  return (speed + a) * W;
+  if constexpr (FAST) {
+    const float ir = frcp<true>(rho);
+    const float u = s.y * ir, v = s.z * ir;
+    const float k = fmaf(v, v, u * u);
+    const float p = fmaf(-0.5f * rho, k, s.w) * (gamma - 1.0f);
+    return (fsqrt<true>(k) + fsqrt<true>(gamma * (p * ir))) * W;
+  } else {
+    float u = s.y / rho, v = s.z / rho;
+    float p = (s.w - 0.5f * rho * (u * u + v * v)) * (gamma - 1.0f);
+    float T = p / rho;
+    float a = sqrtf(gamma * T);
+    float speed = sqrtf(u * u + v * v);
+    return (speed + a) * W;
+  }
 }
 
 // Cell area of the quad a=(i,j), b=(i+1,j), c=(i,j+1), d=(i+1,j+1) (shaders/grid.js:140).

@@ -8,8 +8,8 @@
 // The tile height is a template parameter chosen per solve (or batch) by the autotuner.
 //
 // Geometry comes from the FP64-computed face records (k_metrics_d): Mi[j][i] =
-// (nx, ny, len, 1/A) of the face left of cell (i, j), Mj[j][i] = (nx, ny, len, W) of
-// the face below it, W the cell's wave-speed factor.  A tile stages the records of its
+// (nx, ny, len/2, 1/A) of the face left of cell (i, j), Mj[j][i] = (nx, ny, len/2, W)
+// of the face below it, W the cell's wave-speed factor.  A tile stages the records of its
 // faces in shared memory (Ti: TY rows x 33 faces, Tj: TY+1 rows x 32 faces); the face
 // phase reads a face's record and overwrites it with that face's flux x length, so the
 // flux tiles share that memory.  Each face is read and written by one thread only, and
@@ -113,8 +113,9 @@ __device__ __forceinline__ FaceW own_weights(const float4 (*Ti)[TX + 1], const f
 
 // Flux x length of every face of the tile, written over the face's record.  Face rows
 // ty and ty + TY/2 of each direction per thread; warp 1 also takes the right face
-// column (rows 0..TY-1), warp 0 the top face row.
-template <int SCHEME, int TY>
+// column (rows 0..TY-1), warp 0 the top face row.  INNER: the tile with its halo lies
+// inside the grid away from the seam, so every face exists and no bound is tested.
+template <int SCHEME, int TY, bool INNER = false>
 __device__ __forceinline__ void faces_phase(const float4 (*P)[TX + 4], float4 (*Ti)[TX + 1], float4 (*Tj)[TX],
                                             const Consts& c, int i0, int j0, int M, int N, int tx, int ty) {
   constexpr int NWY = Geo<TY>::NWY, PW = Geo<TY>::PW;
@@ -122,7 +123,7 @@ __device__ __forceinline__ void faces_phase(const float4 (*P)[TX + 4], float4 (*
   for (int t = 0; t < nI; t++) {
     const int r = t < 2 ? ty + NWY * t : tx;
     const int cc = t < 2 ? tx : TX;
-    if (j0 + r < N && cc <= M - i0) {
+    if (INNER || (j0 + r < N && cc <= M - i0)) {
       const float4 m = Ti[r][cc];
       const float4* b = &P[r + 2][cc];
       Ti[r][cc] = face_flux_len<SCHEME>(b[0], b[1], b[2], b[3], m.x, m.y, m.z, c);
@@ -132,7 +133,7 @@ __device__ __forceinline__ void faces_phase(const float4 (*P)[TX + 4], float4 (*
   for (int t = 0; t < nJ; t++) {
     const int r = t < 2 ? ty + NWY * t : TY;
     const int cc = tx;
-    if (j0 + r <= N && i0 + cc < M) {
+    if (INNER || (j0 + r <= N && i0 + cc < M)) {
       const float4 m = Tj[r][cc];
       const float4* b = &P[r][cc + 2];
       Tj[r][cc] = face_flux_len<SCHEME>(b[0], b[PW], b[2 * PW], b[3 * PW], m.x, m.y, m.z, c);
@@ -143,7 +144,7 @@ __device__ __forceinline__ void faces_phase(const float4 (*P)[TX + 4], float4 (*
 // Residual and stage combination of the two owned cells from the face fluxes Fi (over
 // Ti) and Fj (over Tj); returns the max wave-speed bits of the new state when EMIT.
 // qn(h) fetches Qn of owned cell h (stages 2, 3).
-template <int STAGE, bool EMIT, int TY, class QnFetch>
+template <int STAGE, bool EMIT, int TY, bool INNER = false, class QnFetch>
 __device__ __forceinline__ uint32_t combine_phase(const float4 (*Fi)[TX + 1], const float4 (*Fj)[TX], const FaceW& w,
                                                   float4 qa, float4 qb, QnFetch qn, float4* __restrict__ Qo, float dt,
                                                   const Consts& c, int i0, int j0, int M, int N, int tx, int ty) {
@@ -154,7 +155,7 @@ __device__ __forceinline__ uint32_t combine_phase(const float4 (*Fi)[TX + 1], co
   for (int h = 0; h < 2; h++) {
     const int r = ty + NWY * h;
     const int j = j0 + r;
-    if (i < M && j < N) {
+    if (INNER || (i < M && j < N)) {
       const float4 q = h ? qb : qa;
       const float2 niA = make_float2(-w.iA[h], -w.iA[h]), m1 = make_float2(-1.0f, -1.0f);
       const float4 fl = Fi[r][tx], fr = Fi[r][tx + 1], fd = Fj[r][tx], fu = Fj[r + 1][tx];

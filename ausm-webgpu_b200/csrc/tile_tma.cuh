@@ -71,15 +71,15 @@ __device__ __forceinline__ bool tile_tma_wait(unsigned char* smem, int q, int ti
   return true;
 }
 
-// The whole stage of tile (i0, j0); wmax gets the tile's max wave-speed bits (EMIT).
-// Returns false (nothing written) when one of the tile's loads timed out.
-template <int SCHEME, int STAGE, bool EMIT, int TY>
-__device__ __forceinline__ bool tile_tma_body(unsigned char* smem, const CUtensorMap* qs, const CUtensorMap* qn,
-                                              const CUtensorMap* mi, const CUtensorMap* mj,
-                                              const float4* __restrict__ Qs, float4* __restrict__ Qo,
-                                              const float4* __restrict__ Mi, const float4* __restrict__ Mj, float dt,
-                                              const Consts& c, int M, int N, int i0, int j0, int* err,
-                                              uint32_t& wmax) {
+// The tile's compute once its state box has landed: ghost rows, seam columns and
+// conversion to primitives, then (after the face records) the face phase, then (after
+// Qn) the combine.  INNER: tile and halo inside the grid, clear of the seam, so the
+// state box holds every entry and no bound is tested.
+template <int SCHEME, int STAGE, bool EMIT, int TY, bool INNER>
+__device__ __forceinline__ bool tile_tma_compute(unsigned char* smem, const float4* __restrict__ Qs,
+                                                 float4* __restrict__ Qo, const float4* __restrict__ Mi,
+                                                 const float4* __restrict__ Mj, float dt, const Consts& c, int M,
+                                                 int N, int i0, int j0, int* err, uint32_t& wmax) {
   using L = T1<TY>;
   constexpr int NWY = Geo<TY>::NWY, NT = Geo<TY>::NT, HALO = Geo<TY>::HALO;
   float4(*P)[TX + 4] = reinterpret_cast<float4(*)[TX + 4]>(smem);
@@ -87,16 +87,18 @@ __device__ __forceinline__ bool tile_tma_body(unsigned char* smem, const CUtenso
   float4(*Tj)[TX] = reinterpret_cast<float4(*)[TX]>(smem + L::OFF_J);
   float4(*SN)[TX] = reinterpret_cast<float4(*)[TX]>(smem + L::OFF_N);
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * NWX + tx;
-  if (tid == 0) tile_tma_issue<STAGE, TY>(qs, qn, mi, mj, smem, i0, j0);
-  if (!tile_tma_wait<STAGE, TY>(smem, 0, tid, err)) return false;
 
   // fill seam columns and ghost rows the state box could not hold, keep the owned
   // conserved states, convert to primitives in place (the face records are landing)
   auto stage_entry = [&](int pr, int pc) {
-    const int ig = i0 - 2 + pc, j = j0 - 2 + pr;
     float4 q;
-    if (j >= 0 && j < N) q = (ig >= 0 && ig < M) ? P[pr][pc] : __ldg(&Qs[(size_t)j * M + wrap_i(ig, M)]);
-    else q = tile_cell(Qs, Mj, c, M, N, wrap_i(ig, M), j);
+    if constexpr (INNER) {
+      q = P[pr][pc];
+    } else {
+      const int ig = i0 - 2 + pc, j = j0 - 2 + pr;
+      if (j >= 0 && j < N) q = (ig >= 0 && ig < M) ? P[pr][pc] : __ldg(&Qs[(size_t)j * M + wrap_i(ig, M)]);
+      else q = tile_cell(Qs, Mj, c, M, N, wrap_i(ig, M), j);
+    }
     P[pr][pc] = to_prim<true>(q, c.gm1);
     return q;
   };
@@ -112,22 +114,39 @@ __device__ __forceinline__ bool tile_tma_body(unsigned char* smem, const CUtenso
     }
   }
   if (!tile_tma_wait<STAGE, TY>(smem, 1, tid, err)) return false;  // also orders the P writes
-  if (i0 + TX >= M) {  // uniform per CTA: the face column past the seam (zero-filled by the box)
+  if (!INNER && i0 + TX >= M) {  // uniform per CTA: the face column past the seam (zero-filled by the box)
     if (tx == 0)
       for (int r = ty; r < TY; r += NWY)
         if (j0 + r < N) Ti[r][M - i0] = __ldg(&Mi[(size_t)(j0 + r) * M]);
     __syncthreads();
   }
   const FaceW w = own_weights<TY>(Ti, Tj, tx, ty);
-  faces_phase<SCHEME, TY>(P, Ti, Tj, c, i0, j0, M, N, tx, ty);
+  faces_phase<SCHEME, TY, INNER>(P, Ti, Tj, c, i0, j0, M, N, tx, ty);
   if constexpr (STAGE >= 2) {
     if (!tile_tma_wait<STAGE, TY>(smem, 2, tid, err)) return false;  // also orders the flux writes
   } else {
     __syncthreads();
   }
   auto qnf = [&](int h) { return SN[ty + NWY * h][tx]; };
-  wmax = combine_phase<STAGE, EMIT, TY>(Ti, Tj, w, qa, qb, qnf, Qo, dt, c, i0, j0, M, N, tx, ty);
+  wmax = combine_phase<STAGE, EMIT, TY, INNER>(Ti, Tj, w, qa, qb, qnf, Qo, dt, c, i0, j0, M, N, tx, ty);
   return true;
+}
+
+// The whole stage of tile (i0, j0); wmax gets the tile's max wave-speed bits (EMIT).
+// Returns false (nothing written) when one of the tile's loads timed out.
+template <int SCHEME, int STAGE, bool EMIT, int TY>
+__device__ __forceinline__ bool tile_tma_body(unsigned char* smem, const CUtensorMap* qs, const CUtensorMap* qn,
+                                              const CUtensorMap* mi, const CUtensorMap* mj,
+                                              const float4* __restrict__ Qs, float4* __restrict__ Qo,
+                                              const float4* __restrict__ Mi, const float4* __restrict__ Mj, float dt,
+                                              const Consts& c, int M, int N, int i0, int j0, int* err,
+                                              uint32_t& wmax) {
+  const int tid = threadIdx.y * NWX + threadIdx.x;
+  if (tid == 0) tile_tma_issue<STAGE, TY>(qs, qn, mi, mj, smem, i0, j0);
+  if (!tile_tma_wait<STAGE, TY>(smem, 0, tid, err)) return false;
+  const bool inner = i0 >= 2 && i0 + TX + 2 <= M && j0 >= 2 && j0 + TY + 2 <= N;  // uniform per CTA
+  if (inner) return tile_tma_compute<SCHEME, STAGE, EMIT, TY, true>(smem, Qs, Qo, Mi, Mj, dt, c, M, N, i0, j0, err, wmax);
+  return tile_tma_compute<SCHEME, STAGE, EMIT, TY, false>(smem, Qs, Qo, Mi, Mj, dt, c, M, N, i0, j0, err, wmax);
 }
 
 }  // namespace tile
