@@ -119,26 +119,26 @@ template <int SCHEME, int TY, bool INNER = false>
 __device__ __forceinline__ void faces_phase(const float4 (*P)[TX + 4], float4 (*Ti)[TX + 1], float4 (*Tj)[TX],
                                             const Consts& c, int i0, int j0, int M, int N, int tx, int ty) {
   constexpr int NWY = Geo<TY>::NWY, PW = Geo<TY>::PW;
-  const int nI = ty == 1 && tx < TY ? 3 : 2;
-  for (int t = 0; t < nI; t++) {
-    const int r = t < 2 ? ty + NWY * t : tx;
-    const int cc = t < 2 ? tx : TX;
+  auto iface = [&](int r, int cc) {
     if (INNER || (j0 + r < N && cc <= M - i0)) {
       const float4 m = Ti[r][cc];
       const float4* b = &P[r + 2][cc];
       Ti[r][cc] = face_flux_len<SCHEME>(b[0], b[1], b[2], b[3], m.x, m.y, m.z, c);
     }
-  }
-  const int nJ = ty == 0 ? 3 : 2;
-  for (int t = 0; t < nJ; t++) {
-    const int r = t < 2 ? ty + NWY * t : TY;
-    const int cc = tx;
+  };
+  auto jface = [&](int r, int cc) {
     if (INNER || (j0 + r <= N && i0 + cc < M)) {
       const float4 m = Tj[r][cc];
       const float4* b = &P[r][cc + 2];
       Tj[r][cc] = face_flux_len<SCHEME>(b[0], b[PW], b[2 * PW], b[3 * PW], m.x, m.y, m.z, c);
     }
-  }
+  };
+#pragma unroll
+  for (int t = 0; t < 2; t++) iface(ty + NWY * t, tx);
+  if (ty == 1 && tx < TY) iface(tx, TX);
+#pragma unroll
+  for (int t = 0; t < 2; t++) jface(ty + NWY * t, tx);
+  if (ty == 0) jface(TY, tx);
 }
 
 // Residual and stage combination of the two owned cells from the face fluxes Fi (over
