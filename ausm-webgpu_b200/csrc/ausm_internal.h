@@ -98,12 +98,13 @@ struct BatchSolve {
 };
 // All launches go to stream s.  rot: steps already taken since the descriptors' cur.
 // Stage 0 writes the residual dQ/dt of the current state into the solve's next buffer.
-// A stage launch covers one scheme group: descriptors [s_lo, s_hi), items [t_lo, t_hi).
+// A stage launch covers the work items [t_lo, t_hi) of one scheme group; items[t] is the
+// descriptor index of work item t.
 void launch_batch_dt(BatchSolve* d, int nsolves, cudaStream_t s);
 // rows: tile height (8, 16, 32) the descriptors' work items were laid out with.  With
 // err != nullptr (every solve of the launch has maps for that height) stages 1-3 stage
 // their tiles by TMA and a bounded-wait timeout sets *err; without TMA rows must be 16.
-void launch_batch_stage(int scheme, int stage, bool emit, const BatchSolve* d, int s_lo, int s_hi, int t_lo,
+void launch_batch_stage(int scheme, int stage, bool emit, const BatchSolve* d, const int* items, int t_lo,
                         int t_hi, int rot, int rows, int* err, cudaStream_t s);
 void launch_batch_advance(BatchSolve* d, int nsolves, int steps, cudaStream_t s);
 // out[2 s] = dt, out[2 s + 1] = max wave speed of solve s

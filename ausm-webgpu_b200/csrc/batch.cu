@@ -47,6 +47,10 @@ struct ausm_batch {
   int total_tiles = 0;
   int total_chunks = 0;  // residual-norm chunks of all members
   BatchSolve* d_solves = nullptr;
+  std::vector<int> items;  // descriptor index of each work item (the device's d_items)
+  int* d_items = nullptr;
+  int item_cap = 0;
+  bool items_uploaded = false;
   CUtensorMap* d_maps = nullptr;  // 8 per descriptor (halo[3], plain[3], mi, mj) when tma
   bool tma = false;               // every member has tensor maps: stages load tiles by TMA
   int rows = 16;                  // tile height of the work list
@@ -144,6 +148,17 @@ int ensure_capacity(ausm_batch* b) {
     b->cap = cap;
     b->uploaded = false;
   }
+  if (b->total_tiles > b->item_cap) {
+    int cap = std::max(b->total_tiles, 2 * b->item_cap);
+    drop_graphs(b);
+    BCU(b, cudaStreamSynchronize(b->st));
+    cudaFree(b->d_items);
+    b->d_items = nullptr;
+    b->item_cap = 0;
+    BCU(b, cudaMalloc((void**)&b->d_items, cap * sizeof(int)));
+    b->item_cap = cap;
+    b->items_uploaded = false;
+  }
   if (b->total_chunks > b->part_cap) {
     int cap = std::max(b->total_chunks, 2 * b->part_cap);
     BCU(b, cudaStreamSynchronize(b->st));
@@ -170,6 +185,7 @@ void relayout(ausm_batch* b) {
   });
   int t = 0;
   b->groups.clear();
+  b->items.clear();
   b->tma = !b->members.empty();
   for (ausm_solver* h : b->members) b->tma = b->tma && h->tma[0].ok && h->tma[1].ok && h->tma[2].ok;
   if (!b->tma) b->rows = 16;
@@ -180,7 +196,9 @@ void relayout(ausm_batch* b) {
     const int s = (int)b->mirror.size();
     if (b->groups.empty() || b->groups.back().scheme != h->p.scheme) b->groups.push_back({h->p.scheme, s, s, t, t});
     b->mirror.push_back(describe(h, t, chunks, maps_of(b, s)));
-    t += ((h->M + kTX - 1) / kTX) * ((h->N + rows - 1) / rows);
+    const int tiles = ((h->M + kTX - 1) / kTX) * ((h->N + rows - 1) / rows);
+    b->items.insert(b->items.end(), tiles, s);
+    t += tiles;
     chunks += (int)(((size_t)h->M * h->N + kNormChunk - 1) / kNormChunk);
     b->groups.back().s_hi = s + 1;
     b->groups.back().t_hi = t;
@@ -188,6 +206,7 @@ void relayout(ausm_batch* b) {
   b->total_tiles = t;
   b->total_chunks = chunks;
   b->uploaded = false;
+  b->items_uploaded = false;
 }
 
 // Brings the device descriptors up to date with the members' host state.
@@ -224,6 +243,11 @@ int sync_descriptors(ausm_batch* b) {
     }
     b->uploaded = true;
   }
+  if (!b->items_uploaded && !b->items.empty()) {
+    BCU(b, cudaMemcpyAsync(b->d_items, b->items.data(), b->items.size() * sizeof(int), cudaMemcpyHostToDevice,
+                           b->st));
+    b->items_uploaded = true;
+  }
   return AUSM_OK;
 }
 
@@ -242,9 +266,9 @@ void enqueue_steps(ausm_batch* b, int n) {
     const ausm_batch::Group& q = b->groups[g];
     cudaStream_t s = g == 0 ? b->st : b->aux[g - 1];
     for (int k = 0; k < n; k++) {
-      ausm::launch_batch_stage(q.scheme, 1, false, b->d_solves, q.s_lo, q.s_hi, q.t_lo, q.t_hi, k, b->rows, err, s);
-      ausm::launch_batch_stage(q.scheme, 2, false, b->d_solves, q.s_lo, q.s_hi, q.t_lo, q.t_hi, k, b->rows, err, s);
-      ausm::launch_batch_stage(q.scheme, 3, k == n - 1, b->d_solves, q.s_lo, q.s_hi, q.t_lo, q.t_hi, k, b->rows, err,
+      ausm::launch_batch_stage(q.scheme, 1, false, b->d_solves, b->d_items, q.t_lo, q.t_hi, k, b->rows, err, s);
+      ausm::launch_batch_stage(q.scheme, 2, false, b->d_solves, b->d_items, q.t_lo, q.t_hi, k, b->rows, err, s);
+      ausm::launch_batch_stage(q.scheme, 3, k == n - 1, b->d_solves, b->d_items, q.t_lo, q.t_hi, k, b->rows, err,
                                s);
     }
   }
@@ -292,7 +316,7 @@ int tune_rows(ausm_batch* b) {
       if (rc) return rc;
       auto launch = [&] {
         for (const ausm_batch::Group& q : b->groups)
-          ausm::launch_batch_stage(q.scheme, 1, false, b->d_solves, q.s_lo, q.s_hi, q.t_lo, q.t_hi, 0, r, b->d_err,
+          ausm::launch_batch_stage(q.scheme, 1, false, b->d_solves, b->d_items, q.t_lo, q.t_hi, 0, r, b->d_err,
                                    b->st);
       };
       launch();
@@ -389,6 +413,7 @@ int ausm_batch_destroy(ausm_batch* b) {
   if (b->st) cudaStreamSynchronize(b->st);
   drop_graphs(b);
   cudaFree(b->d_solves);
+  cudaFree(b->d_items);
   cudaFree(b->d_maps);
   cudaFree(b->d_err);
   cudaFree(b->d_out);
@@ -506,7 +531,7 @@ int ausm_batch_residual_l2(ausm_batch* b, double* l2) {
   rc = sync_descriptors(b);
   if (rc) return rc;
   for (const ausm_batch::Group& q : b->groups)
-    ausm::launch_batch_stage(q.scheme, 0, false, b->d_solves, q.s_lo, q.s_hi, q.t_lo, q.t_hi, 0, b->rows, nullptr,
+    ausm::launch_batch_stage(q.scheme, 0, false, b->d_solves, b->d_items, q.t_lo, q.t_hi, 0, b->rows, nullptr,
                              b->st);
   ausm::launch_batch_residual_norm(b->d_solves, ns, b->total_chunks, b->d_part, b->d_l2, b->st);
   BCU(b, cudaGetLastError());

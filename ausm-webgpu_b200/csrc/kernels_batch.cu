@@ -1,8 +1,9 @@
 // Batched stage kernel: one launch per RK stage and scheme advances every solve of that
 // scheme in a batch of independent O-grids of any sizes (stage 0: residual only).  The
 // work list is the concatenation of all solves' 32 x TY tiles, grouped by scheme; each
-// CTA takes one work item, finds its solve by binary search over the solves'
-// first-tile offsets, and runs the same tile compute as the single-solve kernel
+// CTA takes one work item, reads its solve's descriptor index from the item table (one
+// load, where a binary search over the first-tile offsets took a chain of dependent
+// loads), and runs the same tile compute as the single-solve kernel
 // (stage_tile.cuh) with that solve's buffers, constants and dt; with TMA (every solve
 // has tensor maps) its boxes are loaded through the solve's maps (tile_tma.cuh).  The
 // tile height TY (8, 16 or 32) is chosen per batch by the autotuner (batch.cu).  The
@@ -22,18 +23,6 @@
 namespace ausm {
 using namespace tile;
 
-// solve owning work item `item` among descriptors [lo, hi): the last whose first tile
-// is <= item
-__device__ __forceinline__ int solve_of(const BatchSolve* __restrict__ solves, int lo, int hi, int item) {
-  hi -= 1;
-  while (lo < hi) {
-    int mid = (lo + hi + 1) >> 1;
-    if (solves[mid].tile0 <= item) lo = mid;
-    else hi = mid - 1;
-  }
-  return lo;
-}
-
 // dynamic shared memory of the per-thread-load kernel: P, Ti, Tj
 template <int TY> struct LdgSmem {
   static constexpr int OFF_I = (TX + 4) * (TY + 4) * 16;
@@ -41,11 +30,11 @@ template <int TY> struct LdgSmem {
   static constexpr int BYTES = OFF_J + (TY + 1) * TX * 16;
 };
 
-// One CTA per work item of one scheme group: item t0 + blockIdx.x, its solve among
-// descriptors [s_lo, s_hi); per-thread loads.
+// One CTA per work item of one scheme group: item t0 + blockIdx.x, its solve
+// descriptor items[item]; per-thread loads.
 template <int SCHEME, int STAGE, bool EMIT, int TY>
 __global__ void __launch_bounds__(Geo<TY>::NT, Geo<TY>::MIN_BLOCKS)
-    k_batch_stage(const BatchSolve* __restrict__ solves, const int s_lo, const int s_hi, const int t0, const int rot) {
+    k_batch_stage(const BatchSolve* __restrict__ solves, const int* __restrict__ items, const int t0, const int rot) {
   using G = Geo<TY>;
   extern __shared__ __align__(16) unsigned char smem_ldg[];  // P, Ti, Tj (LdgSmem<TY>)
   float4(*P)[G::PW] = reinterpret_cast<float4(*)[G::PW]>(smem_ldg);
@@ -53,7 +42,7 @@ __global__ void __launch_bounds__(Geo<TY>::NT, Geo<TY>::MIN_BLOCKS)
   float4(*Tj)[TX] = reinterpret_cast<float4(*)[TX]>(smem_ldg + LdgSmem<TY>::OFF_J);
   const int tx = threadIdx.x, ty = threadIdx.y;
   const int item = t0 + blockIdx.x;
-  const BatchSolve& d = solves[solve_of(solves, s_lo, s_hi, item)];
+  const BatchSolve& d = solves[__ldg(&items[item])];
   const Consts c = d.c;
   const int M = d.M, N = d.N;
   const int local = item - d.tile0;
@@ -77,12 +66,12 @@ __global__ void __launch_bounds__(Geo<TY>::NT, Geo<TY>::MIN_BLOCKS)
 // maps (in global memory, for this tile height).
 template <int SCHEME, int STAGE, bool EMIT, int TY>
 __global__ void __launch_bounds__(Geo<TY>::NT, Geo<TY>::MIN_BLOCKS)
-    k_batch_stage_tma(const BatchSolve* __restrict__ solves, const int s_lo, const int s_hi, const int t0,
+    k_batch_stage_tma(const BatchSolve* __restrict__ solves, const int* __restrict__ items, const int t0,
                       const int rot, int* __restrict__ err) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   unsigned char* smem = smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u);
   const int item = t0 + blockIdx.x;
-  const BatchSolve& d = solves[solve_of(solves, s_lo, s_hi, item)];
+  const BatchSolve& d = solves[__ldg(&items[item])];
   const Consts c = d.c;
   const int M = d.M, N = d.N;
   const int local = item - d.tile0;
@@ -186,7 +175,7 @@ void launch_batch_advance(BatchSolve* d, int nsolves, int steps, cudaStream_t s)
 
 namespace {
 template <int SC, int ST, bool E, int TY>
-void launch_b(const BatchSolve* d, int s_lo, int s_hi, int t_lo, int t_hi, int rot, int* err, cudaStream_t s) {
+void launch_b(const BatchSolve* d, const int* items, int t_lo, int t_hi, int rot, int* err, cudaStream_t s) {
   const dim3 block(NWX, Geo<TY>::NWY);
   if constexpr (ST != 0) {
     if (err) {
@@ -196,7 +185,7 @@ void launch_b(const BatchSolve* d, int s_lo, int s_hi, int t_lo, int t_hi, int r
                              T1<TY>::SMEM);
         attr = true;
       }
-      k_batch_stage_tma<SC, ST, E, TY><<<t_hi - t_lo, block, T1<TY>::SMEM, s>>>(d, s_lo, s_hi, t_lo, rot, err);
+      k_batch_stage_tma<SC, ST, E, TY><<<t_hi - t_lo, block, T1<TY>::SMEM, s>>>(d, items, t_lo, rot, err);
       return;
     }
   }
@@ -208,33 +197,33 @@ void launch_b(const BatchSolve* d, int s_lo, int s_hi, int t_lo, int t_hi, int r
                            LdgSmem<TY>::BYTES);
       attr = true;
     }
-    k_batch_stage<SC, ST, E, TY><<<t_hi - t_lo, block, LdgSmem<TY>::BYTES, s>>>(d, s_lo, s_hi, t_lo, rot);
+    k_batch_stage<SC, ST, E, TY><<<t_hi - t_lo, block, LdgSmem<TY>::BYTES, s>>>(d, items, t_lo, rot);
   }
 }
 template <int SC, int TY>
-void launch_scheme(int stage, bool emit, const BatchSolve* d, int s_lo, int s_hi, int t_lo, int t_hi, int rot,
+void launch_scheme(int stage, bool emit, const BatchSolve* d, const int* items, int t_lo, int t_hi, int rot,
                    int* err, cudaStream_t s) {
-  if (stage == 0) launch_b<SC, 0, false, TY>(d, s_lo, s_hi, t_lo, t_hi, rot, nullptr, s);
-  else if (stage == 1) launch_b<SC, 1, false, TY>(d, s_lo, s_hi, t_lo, t_hi, rot, err, s);
-  else if (stage == 2) launch_b<SC, 2, false, TY>(d, s_lo, s_hi, t_lo, t_hi, rot, err, s);
-  else if (emit) launch_b<SC, 3, true, TY>(d, s_lo, s_hi, t_lo, t_hi, rot, err, s);
-  else launch_b<SC, 3, false, TY>(d, s_lo, s_hi, t_lo, t_hi, rot, err, s);
+  if (stage == 0) launch_b<SC, 0, false, TY>(d, items, t_lo, t_hi, rot, nullptr, s);
+  else if (stage == 1) launch_b<SC, 1, false, TY>(d, items, t_lo, t_hi, rot, err, s);
+  else if (stage == 2) launch_b<SC, 2, false, TY>(d, items, t_lo, t_hi, rot, err, s);
+  else if (emit) launch_b<SC, 3, true, TY>(d, items, t_lo, t_hi, rot, err, s);
+  else launch_b<SC, 3, false, TY>(d, items, t_lo, t_hi, rot, err, s);
 }
 template <int TY>
-void launch_rows(int scheme, int stage, bool emit, const BatchSolve* d, int s_lo, int s_hi, int t_lo, int t_hi,
+void launch_rows(int scheme, int stage, bool emit, const BatchSolve* d, const int* items, int t_lo, int t_hi,
                  int rot, int* err, cudaStream_t s) {
-  if (scheme == 0) launch_scheme<0, TY>(stage, emit, d, s_lo, s_hi, t_lo, t_hi, rot, err, s);
-  else if (scheme == 1) launch_scheme<1, TY>(stage, emit, d, s_lo, s_hi, t_lo, t_hi, rot, err, s);
-  else launch_scheme<2, TY>(stage, emit, d, s_lo, s_hi, t_lo, t_hi, rot, err, s);
+  if (scheme == 0) launch_scheme<0, TY>(stage, emit, d, items, t_lo, t_hi, rot, err, s);
+  else if (scheme == 1) launch_scheme<1, TY>(stage, emit, d, items, t_lo, t_hi, rot, err, s);
+  else launch_scheme<2, TY>(stage, emit, d, items, t_lo, t_hi, rot, err, s);
 }
 }  // namespace
 
-void launch_batch_stage(int scheme, int stage, bool emit, const BatchSolve* d, int s_lo, int s_hi, int t_lo,
+void launch_batch_stage(int scheme, int stage, bool emit, const BatchSolve* d, const int* items, int t_lo,
                         int t_hi, int rot, int rows, int* err, cudaStream_t s) {
   if (t_hi <= t_lo) return;
-  if (rows == 8) launch_rows<8>(scheme, stage, emit, d, s_lo, s_hi, t_lo, t_hi, rot, err, s);
-  else if (rows == 32) launch_rows<32>(scheme, stage, emit, d, s_lo, s_hi, t_lo, t_hi, rot, err, s);
-  else launch_rows<16>(scheme, stage, emit, d, s_lo, s_hi, t_lo, t_hi, rot, err, s);
+  if (rows == 8) launch_rows<8>(scheme, stage, emit, d, items, t_lo, t_hi, rot, err, s);
+  else if (rows == 32) launch_rows<32>(scheme, stage, emit, d, items, t_lo, t_hi, rot, err, s);
+  else launch_rows<16>(scheme, stage, emit, d, items, t_lo, t_hi, rot, err, s);
 }
 
 }  // namespace ausm
