@@ -96,17 +96,25 @@ struct BatchSolve {
   int M, N, scheme, tiles_x, tile0, cur;
   int chunk0;  // first residual-norm chunk (512 cells) of the solve
 };
+// One work item (tile) of a batch: its solve's descriptor index, that solve's buffer
+// rotation when the table was written, and the tile's column and row.
+struct alignas(16) BatchItem {
+  int solve, cur, ti, tj;
+};
 // All launches go to stream s.  rot: steps already taken since the descriptors' cur.
 // Stage 0 writes the residual dQ/dt of the current state into the solve's next buffer.
-// A stage launch covers the work items [t_lo, t_hi) of one scheme group; items[t] is the
-// descriptor index of work item t.
+// A stage launch covers the work items [t_lo, t_hi) of one scheme group; *steps counts
+// the steps the batch has taken since the item table was written (so a solve's current
+// buffer is (items[t].cur + *steps + rot) % 3); maps holds 8 tensor maps per descriptor.
 void launch_batch_dt(BatchSolve* d, int nsolves, cudaStream_t s);
 // rows: tile height (8, 16, 32) the descriptors' work items were laid out with.  With
 // err != nullptr (every solve of the launch has maps for that height) stages 1-3 stage
 // their tiles by TMA and a bounded-wait timeout sets *err; without TMA rows must be 16.
-void launch_batch_stage(int scheme, int stage, bool emit, const BatchSolve* d, const int* items, int t_lo,
-                        int t_hi, int rot, int rows, int* err, cudaStream_t s);
-void launch_batch_advance(BatchSolve* d, int nsolves, int steps, cudaStream_t s);
+void launch_batch_stage(int scheme, int stage, bool emit, const BatchSolve* d, const BatchItem* items,
+                        const int* steps, const CUtensorMap* maps, int t_lo, int t_hi, int rot, int rows, int* err,
+                        cudaStream_t s);
+// advances every descriptor's cur and the batch's step counter *taken by `steps`
+void launch_batch_advance(BatchSolve* d, int nsolves, int steps, int* taken, cudaStream_t s);
 // out[2 s] = dt, out[2 s + 1] = max wave speed of solve s
 void launch_batch_gather(const BatchSolve* d, int nsolves, float* out, cudaStream_t s);
 // l2[s] = sqrt(mean over solve s's cells of (d rho / dt)^2), from the stage-0 residual;

@@ -47,10 +47,10 @@ struct ausm_batch {
   int total_tiles = 0;
   int total_chunks = 0;  // residual-norm chunks of all members
   BatchSolve* d_solves = nullptr;
-  std::vector<int> items;  // descriptor index of each work item (the device's d_items)
-  int* d_items = nullptr;
+  std::vector<ausm::BatchItem> items;  // the work items (the device's d_items)
+  ausm::BatchItem* d_items = nullptr;
   int item_cap = 0;
-  bool items_uploaded = false;
+  int* d_steps = nullptr;  // steps taken since the item table was uploaded (d_err + 1)
   CUtensorMap* d_maps = nullptr;  // 8 per descriptor (halo[3], plain[3], mi, mj) when tma
   bool tma = false;               // every member has tensor maps: stages load tiles by TMA
   int rows = 16;                  // tile height of the work list
@@ -155,9 +155,9 @@ int ensure_capacity(ausm_batch* b) {
     cudaFree(b->d_items);
     b->d_items = nullptr;
     b->item_cap = 0;
-    BCU(b, cudaMalloc((void**)&b->d_items, cap * sizeof(int)));
+    BCU(b, cudaMalloc((void**)&b->d_items, cap * sizeof(ausm::BatchItem)));
     b->item_cap = cap;
-    b->items_uploaded = false;
+    b->uploaded = false;
   }
   if (b->total_chunks > b->part_cap) {
     int cap = std::max(b->total_chunks, 2 * b->part_cap);
@@ -196,8 +196,8 @@ void relayout(ausm_batch* b) {
     const int s = (int)b->mirror.size();
     if (b->groups.empty() || b->groups.back().scheme != h->p.scheme) b->groups.push_back({h->p.scheme, s, s, t, t});
     b->mirror.push_back(describe(h, t, chunks, maps_of(b, s)));
-    const int tiles = ((h->M + kTX - 1) / kTX) * ((h->N + rows - 1) / rows);
-    b->items.insert(b->items.end(), tiles, s);
+    const int tx = (h->M + kTX - 1) / kTX, tiles = tx * ((h->N + rows - 1) / rows);
+    for (int k = 0; k < tiles; k++) b->items.push_back({s, 0, k % tx, k / tx});
     t += tiles;
     chunks += (int)(((size_t)h->M * h->N + kNormChunk - 1) / kNormChunk);
     b->groups.back().s_hi = s + 1;
@@ -206,7 +206,6 @@ void relayout(ausm_batch* b) {
   b->total_tiles = t;
   b->total_chunks = chunks;
   b->uploaded = false;
-  b->items_uploaded = false;
 }
 
 // Brings the device descriptors up to date with the members' host state.
@@ -241,12 +240,12 @@ int sync_descriptors(ausm_batch* b) {
       BCU(b, cudaMemcpyAsync(b->d_maps, maps.data(), maps.size() * sizeof(CUtensorMap), cudaMemcpyHostToDevice,
                              b->st));
     }
+    // the item table with each solve's current rotation, and the step count restarted
+    for (ausm::BatchItem& it : b->items) it.cur = b->mirror[it.solve].cur;
+    BCU(b, cudaMemcpyAsync(b->d_items, b->items.data(), b->items.size() * sizeof(ausm::BatchItem),
+                           cudaMemcpyHostToDevice, b->st));
+    BCU(b, cudaMemsetAsync(b->d_steps, 0, sizeof(int), b->st));
     b->uploaded = true;
-  }
-  if (!b->items_uploaded && !b->items.empty()) {
-    BCU(b, cudaMemcpyAsync(b->d_items, b->items.data(), b->items.size() * sizeof(int), cudaMemcpyHostToDevice,
-                           b->st));
-    b->items_uploaded = true;
   }
   return AUSM_OK;
 }
@@ -266,9 +265,9 @@ void enqueue_steps(ausm_batch* b, int n) {
     const ausm_batch::Group& q = b->groups[g];
     cudaStream_t s = g == 0 ? b->st : b->aux[g - 1];
     for (int k = 0; k < n; k++) {
-      ausm::launch_batch_stage(q.scheme, 1, false, b->d_solves, b->d_items, q.t_lo, q.t_hi, k, b->rows, err, s);
-      ausm::launch_batch_stage(q.scheme, 2, false, b->d_solves, b->d_items, q.t_lo, q.t_hi, k, b->rows, err, s);
-      ausm::launch_batch_stage(q.scheme, 3, k == n - 1, b->d_solves, b->d_items, q.t_lo, q.t_hi, k, b->rows, err,
+      ausm::launch_batch_stage(q.scheme, 1, false, b->d_solves, b->d_items, b->d_steps, b->d_maps, q.t_lo, q.t_hi, k, b->rows, err, s);
+      ausm::launch_batch_stage(q.scheme, 2, false, b->d_solves, b->d_items, b->d_steps, b->d_maps, q.t_lo, q.t_hi, k, b->rows, err, s);
+      ausm::launch_batch_stage(q.scheme, 3, k == n - 1, b->d_solves, b->d_items, b->d_steps, b->d_maps, q.t_lo, q.t_hi, k, b->rows, err,
                                s);
     }
   }
@@ -276,7 +275,7 @@ void enqueue_steps(ausm_batch* b, int n) {
     cudaEventRecord(b->join[g - 1], b->aux[g - 1]);
     cudaStreamWaitEvent(b->st, b->join[g - 1], 0);
   }
-  ausm::launch_batch_advance(b->d_solves, ns, n, b->st);
+  ausm::launch_batch_advance(b->d_solves, ns, n, b->d_steps, b->st);
   ausm::launch_batch_gather(b->d_solves, ns, b->d_out, b->st);
 }
 
@@ -316,7 +315,7 @@ int tune_rows(ausm_batch* b) {
       if (rc) return rc;
       auto launch = [&] {
         for (const ausm_batch::Group& q : b->groups)
-          ausm::launch_batch_stage(q.scheme, 1, false, b->d_solves, b->d_items, q.t_lo, q.t_hi, 0, r, b->d_err,
+          ausm::launch_batch_stage(q.scheme, 1, false, b->d_solves, b->d_items, b->d_steps, b->d_maps, q.t_lo, q.t_hi, 0, r, b->d_err,
                                    b->st);
       };
       launch();
@@ -402,6 +401,7 @@ int ausm_batch_create(ausm_batch** out) {
   if (e != cudaSuccess) return bail(e, "cudaEventCreate");
   if ((e = cudaMalloc((void**)&b->d_err, 2 * sizeof(int))) != cudaSuccess) return bail(e, "cudaMalloc");
   if ((e = cudaMemsetAsync(b->d_err, 0, 2 * sizeof(int), b->st)) != cudaSuccess) return bail(e, "cudaMemsetAsync");
+  b->d_steps = b->d_err + 1;
   *out = b;
   return AUSM_OK;
 }
@@ -531,7 +531,7 @@ int ausm_batch_residual_l2(ausm_batch* b, double* l2) {
   rc = sync_descriptors(b);
   if (rc) return rc;
   for (const ausm_batch::Group& q : b->groups)
-    ausm::launch_batch_stage(q.scheme, 0, false, b->d_solves, b->d_items, q.t_lo, q.t_hi, 0, b->rows, nullptr,
+    ausm::launch_batch_stage(q.scheme, 0, false, b->d_solves, b->d_items, b->d_steps, b->d_maps, q.t_lo, q.t_hi, 0, b->rows, nullptr,
                              b->st);
   ausm::launch_batch_residual_norm(b->d_solves, ns, b->total_chunks, b->d_part, b->d_l2, b->st);
   BCU(b, cudaGetLastError());

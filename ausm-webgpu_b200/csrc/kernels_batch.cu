@@ -1,9 +1,11 @@
 // Batched stage kernel: one launch per RK stage and scheme advances every solve of that
 // scheme in a batch of independent O-grids of any sizes (stage 0: residual only).  The
 // work list is the concatenation of all solves' 32 x TY tiles, grouped by scheme; each
-// CTA takes one work item, reads its solve's descriptor index from the item table (one
-// load, where a binary search over the first-tile offsets took a chain of dependent
-// loads), and runs the same tile compute as the single-solve kernel
+// CTA takes one work item, reads its solve, the solve's buffer rotation and its tile
+// coordinates from the item table (one load; a binary search over the first-tile
+// offsets took a chain of dependent loads), issues its TMA boxes through the solve's
+// tensor maps before it reads anything else of the solve's descriptor, and runs the
+// same tile compute as the single-solve kernel
 // (stage_tile.cuh) with that solve's buffers, constants and dt; with TMA (every solve
 // has tensor maps) its boxes are loaded through the solve's maps (tile_tma.cuh).  The
 // tile height TY (8, 16 or 32) is chosen per batch by the autotuner (batch.cu).  The
@@ -30,24 +32,35 @@ template <int TY> struct LdgSmem {
   static constexpr int BYTES = OFF_J + (TY + 1) * TX * 16;
 };
 
-// One CTA per work item of one scheme group: item t0 + blockIdx.x, its solve
-// descriptor items[item]; per-thread loads.
+// Work item t0 + blockIdx.x of the item table: its solve, the index of the solve's
+// current buffer and its tile origin.  The buffer index is the solve's rotation when
+// the table was written plus the steps the batch has taken since (*steps) plus rot.
+struct ItemTile {
+  int s, a, i0, j0;
+};
+template <int TY>
+__device__ __forceinline__ ItemTile item_tile(const BatchItem* __restrict__ items, const int* __restrict__ steps,
+                                              int item, int rot) {
+  const BatchItem it = items[item];
+  return {it.solve, (it.cur + *steps + rot) % 3, (int)it.ti * TX, (int)it.tj * TY};
+}
+
+// One CTA per work item of one scheme group; per-thread loads.
 template <int SCHEME, int STAGE, bool EMIT, int TY>
 __global__ void __launch_bounds__(Geo<TY>::NT, Geo<TY>::MIN_BLOCKS)
-    k_batch_stage(const BatchSolve* __restrict__ solves, const int* __restrict__ items, const int t0, const int rot) {
+    k_batch_stage(const BatchSolve* __restrict__ solves, const BatchItem* __restrict__ items,
+                  const int* __restrict__ steps, const int t0, const int rot) {
   using G = Geo<TY>;
   extern __shared__ __align__(16) unsigned char smem_ldg[];  // P, Ti, Tj (LdgSmem<TY>)
   float4(*P)[G::PW] = reinterpret_cast<float4(*)[G::PW]>(smem_ldg);
   float4(*Ti)[TX + 1] = reinterpret_cast<float4(*)[TX + 1]>(smem_ldg + LdgSmem<TY>::OFF_I);
   float4(*Tj)[TX] = reinterpret_cast<float4(*)[TX]>(smem_ldg + LdgSmem<TY>::OFF_J);
   const int tx = threadIdx.x, ty = threadIdx.y;
-  const int item = t0 + blockIdx.x;
-  const BatchSolve& d = solves[__ldg(&items[item])];
+  const ItemTile w0 = item_tile<TY>(items, steps, t0 + blockIdx.x, rot);
+  const BatchSolve& d = solves[w0.s];
   const Consts c = d.c;
-  const int M = d.M, N = d.N;
-  const int local = item - d.tile0;
-  const int i0 = (local % d.tiles_x) * TX, j0 = (local / d.tiles_x) * TY;
-  const int a = (d.cur + rot) % 3, b = (a + 1) % 3, c3 = (a + 2) % 3;
+  const int M = d.M, N = d.N, i0 = w0.i0, j0 = w0.j0;
+  const int a = w0.a, b = (a + 1) % 3, c3 = (a + 2) % 3;
   const float4* Qs = d.Q[STAGE <= 1 ? a : (STAGE == 2 ? b : c3)];
   const float4* Qn = d.Q[a];
   float4* Qo = d.Q[STAGE == 2 ? c3 : b];
@@ -63,26 +76,25 @@ __global__ void __launch_bounds__(Geo<TY>::NT, Geo<TY>::MIN_BLOCKS)
 }
 
 // TMA-staged form (stages 1-3): the tile's boxes come through the solve's own tensor
-// maps (in global memory, for this tile height).
+// maps (in global memory, 8 per solve in descriptor order, for this tile height).
 template <int SCHEME, int STAGE, bool EMIT, int TY>
 __global__ void __launch_bounds__(Geo<TY>::NT, Geo<TY>::MIN_BLOCKS)
-    k_batch_stage_tma(const BatchSolve* __restrict__ solves, const int* __restrict__ items, const int t0,
+    k_batch_stage_tma(const BatchSolve* __restrict__ solves, const BatchItem* __restrict__ items,
+                      const int* __restrict__ steps, const CUtensorMap* __restrict__ maps, const int t0,
                       const int rot, int* __restrict__ err) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   unsigned char* smem = smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u);
-  const int item = t0 + blockIdx.x;
-  const BatchSolve& d = solves[__ldg(&items[item])];
-  const Consts c = d.c;
-  const int M = d.M, N = d.N;
-  const int local = item - d.tile0;
-  const int i0 = (local % d.tiles_x) * TX, j0 = (local / d.tiles_x) * TY;
-  const int a = (d.cur + rot) % 3, b = (a + 1) % 3, c3 = (a + 2) % 3;
+  const ItemTile w0 = item_tile<TY>(items, steps, t0 + blockIdx.x, rot);
+  const int a = w0.a, b = (a + 1) % 3, c3 = (a + 2) % 3;
   const int s_in = STAGE == 1 ? a : (STAGE == 2 ? b : c3);
-  const CUtensorMap* mp = d.maps;
+  const CUtensorMap* mp = maps + 8 * (size_t)w0.s;
+  if (threadIdx.y * NWX + threadIdx.x == 0)
+    tile_tma_issue<STAGE, TY>(&mp[s_in], &mp[3 + a], &mp[6], &mp[7], smem, w0.i0, w0.j0);
+  const BatchSolve& d = solves[w0.s];  // read while the boxes land
+  const Consts c = d.c;
   uint32_t wmax = 0u;
-  if (!tile_tma_body<SCHEME, STAGE, EMIT, TY>(smem, &mp[s_in], &mp[3 + a], &mp[6], &mp[7], d.Q[s_in],
-                                              d.Q[STAGE == 2 ? c3 : b], d.Mi, d.Mj, *d.dt, c, M, N, i0, j0, err,
-                                              wmax))
+  if (!tile_tma_run<SCHEME, STAGE, EMIT, TY>(smem, d.Q[s_in], d.Q[STAGE == 2 ? c3 : b], d.Mi, d.Mj, *d.dt, c, d.M,
+                                             d.N, w0.i0, w0.j0, err, wmax))
     return;
   if constexpr (EMIT) block_max_to(d.wave, wmax);
 }
@@ -96,9 +108,10 @@ __global__ void k_batch_dt(BatchSolve* __restrict__ solves, int n) {
   d.dt[0] = fminf(d.c.maxdt, d.c.cfl / __uint_as_float(d.wave[0]));
   d.wave[0] = 0u;
 }
-__global__ void k_batch_advance(BatchSolve* __restrict__ solves, int n, int steps) {
+__global__ void k_batch_advance(BatchSolve* __restrict__ solves, int n, int steps, int* __restrict__ taken) {
   int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s < n) solves[s].cur = (solves[s].cur + steps) % 3;
+  if (s == 0) *taken += steps;
 }
 
 __global__ void k_batch_gather(const BatchSolve* __restrict__ solves, int n, float* __restrict__ out) {
@@ -169,13 +182,13 @@ void launch_batch_residual_norm(const BatchSolve* d, int nsolves, int total_chun
 void launch_batch_dt(BatchSolve* d, int nsolves, cudaStream_t s) {
   k_batch_dt<<<(nsolves + 127) / 128, 128, 0, s>>>(d, nsolves);
 }
-void launch_batch_advance(BatchSolve* d, int nsolves, int steps, cudaStream_t s) {
-  k_batch_advance<<<(nsolves + 127) / 128, 128, 0, s>>>(d, nsolves, steps);
+void launch_batch_advance(BatchSolve* d, int nsolves, int steps, int* taken, cudaStream_t s) {
+  k_batch_advance<<<(nsolves + 127) / 128, 128, 0, s>>>(d, nsolves, steps, taken);
 }
 
 namespace {
 template <int SC, int ST, bool E, int TY>
-void launch_b(const BatchSolve* d, const int* items, int t_lo, int t_hi, int rot, int* err, cudaStream_t s) {
+void launch_b(const BatchSolve* d, const BatchItem* items, const int* steps, const CUtensorMap* maps, int t_lo, int t_hi, int rot, int* err, cudaStream_t s) {
   const dim3 block(NWX, Geo<TY>::NWY);
   if constexpr (ST != 0) {
     if (err) {
@@ -185,7 +198,7 @@ void launch_b(const BatchSolve* d, const int* items, int t_lo, int t_hi, int rot
                              T1<TY>::SMEM);
         attr = true;
       }
-      k_batch_stage_tma<SC, ST, E, TY><<<t_hi - t_lo, block, T1<TY>::SMEM, s>>>(d, items, t_lo, rot, err);
+      k_batch_stage_tma<SC, ST, E, TY><<<t_hi - t_lo, block, T1<TY>::SMEM, s>>>(d, items, steps, maps, t_lo, rot, err);
       return;
     }
   }
@@ -197,33 +210,34 @@ void launch_b(const BatchSolve* d, const int* items, int t_lo, int t_hi, int rot
                            LdgSmem<TY>::BYTES);
       attr = true;
     }
-    k_batch_stage<SC, ST, E, TY><<<t_hi - t_lo, block, LdgSmem<TY>::BYTES, s>>>(d, items, t_lo, rot);
+    k_batch_stage<SC, ST, E, TY><<<t_hi - t_lo, block, LdgSmem<TY>::BYTES, s>>>(d, items, steps, t_lo, rot);
   }
 }
 template <int SC, int TY>
-void launch_scheme(int stage, bool emit, const BatchSolve* d, const int* items, int t_lo, int t_hi, int rot,
+void launch_scheme(int stage, bool emit, const BatchSolve* d, const BatchItem* items, const int* steps, const CUtensorMap* maps, int t_lo, int t_hi, int rot,
                    int* err, cudaStream_t s) {
-  if (stage == 0) launch_b<SC, 0, false, TY>(d, items, t_lo, t_hi, rot, nullptr, s);
-  else if (stage == 1) launch_b<SC, 1, false, TY>(d, items, t_lo, t_hi, rot, err, s);
-  else if (stage == 2) launch_b<SC, 2, false, TY>(d, items, t_lo, t_hi, rot, err, s);
-  else if (emit) launch_b<SC, 3, true, TY>(d, items, t_lo, t_hi, rot, err, s);
-  else launch_b<SC, 3, false, TY>(d, items, t_lo, t_hi, rot, err, s);
+  if (stage == 0) launch_b<SC, 0, false, TY>(d, items, steps, maps, t_lo, t_hi, rot, nullptr, s);
+  else if (stage == 1) launch_b<SC, 1, false, TY>(d, items, steps, maps, t_lo, t_hi, rot, err, s);
+  else if (stage == 2) launch_b<SC, 2, false, TY>(d, items, steps, maps, t_lo, t_hi, rot, err, s);
+  else if (emit) launch_b<SC, 3, true, TY>(d, items, steps, maps, t_lo, t_hi, rot, err, s);
+  else launch_b<SC, 3, false, TY>(d, items, steps, maps, t_lo, t_hi, rot, err, s);
 }
 template <int TY>
-void launch_rows(int scheme, int stage, bool emit, const BatchSolve* d, const int* items, int t_lo, int t_hi,
+void launch_rows(int scheme, int stage, bool emit, const BatchSolve* d, const BatchItem* items, const int* steps, const CUtensorMap* maps, int t_lo, int t_hi,
                  int rot, int* err, cudaStream_t s) {
-  if (scheme == 0) launch_scheme<0, TY>(stage, emit, d, items, t_lo, t_hi, rot, err, s);
-  else if (scheme == 1) launch_scheme<1, TY>(stage, emit, d, items, t_lo, t_hi, rot, err, s);
-  else launch_scheme<2, TY>(stage, emit, d, items, t_lo, t_hi, rot, err, s);
+  if (scheme == 0) launch_scheme<0, TY>(stage, emit, d, items, steps, maps, t_lo, t_hi, rot, err, s);
+  else if (scheme == 1) launch_scheme<1, TY>(stage, emit, d, items, steps, maps, t_lo, t_hi, rot, err, s);
+  else launch_scheme<2, TY>(stage, emit, d, items, steps, maps, t_lo, t_hi, rot, err, s);
 }
 }  // namespace
 
-void launch_batch_stage(int scheme, int stage, bool emit, const BatchSolve* d, const int* items, int t_lo,
+void launch_batch_stage(int scheme, int stage, bool emit, const BatchSolve* d, const BatchItem* items,
+                        const int* steps, const CUtensorMap* maps, int t_lo,
                         int t_hi, int rot, int rows, int* err, cudaStream_t s) {
   if (t_hi <= t_lo) return;
-  if (rows == 8) launch_rows<8>(scheme, stage, emit, d, items, t_lo, t_hi, rot, err, s);
-  else if (rows == 32) launch_rows<32>(scheme, stage, emit, d, items, t_lo, t_hi, rot, err, s);
-  else launch_rows<16>(scheme, stage, emit, d, items, t_lo, t_hi, rot, err, s);
+  if (rows == 8) launch_rows<8>(scheme, stage, emit, d, items, steps, maps, t_lo, t_hi, rot, err, s);
+  else if (rows == 32) launch_rows<32>(scheme, stage, emit, d, items, steps, maps, t_lo, t_hi, rot, err, s);
+  else launch_rows<16>(scheme, stage, emit, d, items, steps, maps, t_lo, t_hi, rot, err, s);
 }
 
 }  // namespace ausm

@@ -132,8 +132,22 @@ __device__ __forceinline__ bool tile_tma_compute(unsigned char* smem, const floa
   return true;
 }
 
-// The whole stage of tile (i0, j0); wmax gets the tile's max wave-speed bits (EMIT).
-// Returns false (nothing written) when one of the tile's loads timed out.
+// The stage of tile (i0, j0) after thread 0 has issued its loads (tile_tma_issue);
+// wmax gets the tile's max wave-speed bits (EMIT).  Returns false (nothing written)
+// when one of the tile's loads timed out.
+template <int SCHEME, int STAGE, bool EMIT, int TY>
+__device__ __forceinline__ bool tile_tma_run(unsigned char* smem, const float4* __restrict__ Qs,
+                                             float4* __restrict__ Qo, const float4* __restrict__ Mi,
+                                             const float4* __restrict__ Mj, float dt, const Consts& c, int M, int N,
+                                             int i0, int j0, int* err, uint32_t& wmax) {
+  const int tid = threadIdx.y * NWX + threadIdx.x;
+  if (!tile_tma_wait<STAGE, TY>(smem, 0, tid, err)) return false;
+  const bool inner = i0 >= 2 && i0 + TX + 2 <= M && j0 >= 2 && j0 + TY + 2 <= N;  // uniform per CTA
+  if (inner) return tile_tma_compute<SCHEME, STAGE, EMIT, TY, true>(smem, Qs, Qo, Mi, Mj, dt, c, M, N, i0, j0, err, wmax);
+  return tile_tma_compute<SCHEME, STAGE, EMIT, TY, false>(smem, Qs, Qo, Mi, Mj, dt, c, M, N, i0, j0, err, wmax);
+}
+
+// The whole stage of tile (i0, j0): issue, then tile_tma_run.
 template <int SCHEME, int STAGE, bool EMIT, int TY>
 __device__ __forceinline__ bool tile_tma_body(unsigned char* smem, const CUtensorMap* qs, const CUtensorMap* qn,
                                               const CUtensorMap* mi, const CUtensorMap* mj,
@@ -141,12 +155,8 @@ __device__ __forceinline__ bool tile_tma_body(unsigned char* smem, const CUtenso
                                               const float4* __restrict__ Mi, const float4* __restrict__ Mj, float dt,
                                               const Consts& c, int M, int N, int i0, int j0, int* err,
                                               uint32_t& wmax) {
-  const int tid = threadIdx.y * NWX + threadIdx.x;
-  if (tid == 0) tile_tma_issue<STAGE, TY>(qs, qn, mi, mj, smem, i0, j0);
-  if (!tile_tma_wait<STAGE, TY>(smem, 0, tid, err)) return false;
-  const bool inner = i0 >= 2 && i0 + TX + 2 <= M && j0 >= 2 && j0 + TY + 2 <= N;  // uniform per CTA
-  if (inner) return tile_tma_compute<SCHEME, STAGE, EMIT, TY, true>(smem, Qs, Qo, Mi, Mj, dt, c, M, N, i0, j0, err, wmax);
-  return tile_tma_compute<SCHEME, STAGE, EMIT, TY, false>(smem, Qs, Qo, Mi, Mj, dt, c, M, N, i0, j0, err, wmax);
+  if (threadIdx.y * NWX + threadIdx.x == 0) tile_tma_issue<STAGE, TY>(qs, qn, mi, mj, smem, i0, j0);
+  return tile_tma_run<SCHEME, STAGE, EMIT, TY>(smem, Qs, Qo, Mi, Mj, dt, c, M, N, i0, j0, err, wmax);
 }
 
 }  // namespace tile
