@@ -123,7 +123,7 @@ int tuned_tile_rows(ausm_solver* h, bool force, int* rows) {
     for (int k = 0; k < 3; k++) {
       const TmaMaps& tm = h->tma[k];
       if (!tm.ok) continue;
-      const TmaMapsLaunch t = {tm.halo[a], tm.plain[a], tm.mi, tm.mj};
+      const TmaMapsLaunch t = {tm.halo[a], tm.plain[a], tm.mi, tm.mj, tm.wrap[a]};
       auto launch = [&] {
         launch_fused_stage(h->p.scheme, 1, false, h->Q[a], nullptr, h->Q[b], h->Mi, h->Mj, h->dt, h->wave, h->c,
                            h->M, h->N, &t, kTileHeights[k], h->err_flag, h->st);
@@ -797,9 +797,9 @@ int ausm_step(ausm_solver* h, int n, float* dt_out) {
         const TmaMapsLaunch *p1 = nullptr, *p2 = nullptr, *p3 = nullptr;
         const TmaMaps& tm = h->tma[tile_index(rows)];
         if (tm.ok) {
-          t1 = {tm.halo[a], tm.plain[a], tm.mi, tm.mj};
-          t2 = {tm.halo[b], tm.plain[a], tm.mi, tm.mj};
-          t3 = {tm.halo[c3], tm.plain[a], tm.mi, tm.mj};
+          t1 = {tm.halo[a], tm.plain[a], tm.mi, tm.mj, tm.wrap[a]};
+          t2 = {tm.halo[b], tm.plain[a], tm.mi, tm.mj, tm.wrap[b]};
+          t3 = {tm.halo[c3], tm.plain[a], tm.mi, tm.mj, tm.wrap[c3]};
           p1 = &t1; p2 = &t2; p3 = &t3;
         }
         launch_fused_stage(sch, 1, false, h->Q[a], nullptr, h->Q[b], h->Mi, h->Mj, h->dt, h->wave, h->c, M, N, p1,

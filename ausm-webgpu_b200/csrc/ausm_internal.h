@@ -51,19 +51,22 @@ __device__ __forceinline__ void block_sum_store(double* dst, double v) {
 constexpr int kMaxParts = 148 * 16;
 
 // ---- fused engine (kernels_fused.cu) ----
-// TMA descriptors of one solve: per state buffer the halo box (36 x 20 cells) and the
-// plain box (32 x 16 cells), and the face-record boxes (33 x 16 i-faces, 32 x 17
-// j-faces).
+// TMA descriptors of one solve for one tile height ty: per state buffer the halo box
+// (36 x (ty+4) cells), the plain box (32 x ty cells) and the seam box (2 x (ty+4)
+// cells: the two columns a tile at the seam wraps to), and the face-record boxes
+// (33 x ty i-faces, 32 x (ty+1) j-faces).
 struct TmaMaps {
   CUtensorMap halo[3];
   CUtensorMap plain[3];
   CUtensorMap mi, mj;
+  CUtensorMap wrap[3];
   bool ok = false;
 };
-struct TmaMapsLaunch {  // the four a stage launch reads
+struct TmaMapsLaunch {  // the five a stage launch reads
   CUtensorMap qs;
   CUtensorMap qn;
   CUtensorMap mi, mj;
+  CUtensorMap wrap;  // seam box of the buffer qs reads
 };
 // Tile heights of the TMA tile kernels (the autotuner's candidates) and their index.
 constexpr int kTileHeights[3] = {8, 16, 32};
@@ -96,16 +99,21 @@ struct BatchSolve {
   int M, N, scheme, tiles_x, tile0, cur;
   int chunk0;  // first residual-norm chunk (512 cells) of the solve
 };
+// Tensor maps per batch member, in this order: halo[0..2], plain[0..2], mi, mj,
+// wrap[0..2] (TmaMaps of the batch's tile height).
+constexpr int kBatchMaps = 11;
 // One work item (tile) of a batch: its solve's descriptor index, that solve's buffer
-// rotation when the table was written, and the tile's column and row.
+// rotation when the table was written, the tile's column | row << 16, and the solve's
+// M (what the tile's loads need, in one 16-byte load).
 struct alignas(16) BatchItem {
-  int solve, cur, ti, tj;
+  int solve, cur, tile, M;
 };
 // All launches go to stream s.  rot: steps already taken since the descriptors' cur.
 // Stage 0 writes the residual dQ/dt of the current state into the solve's next buffer.
 // A stage launch covers the work items [t_lo, t_hi) of one scheme group; *steps counts
 // the steps the batch has taken since the item table was written (so a solve's current
-// buffer is (items[t].cur + *steps + rot) % 3); maps holds 8 tensor maps per descriptor.
+// buffer is (items[t].cur + *steps + rot) % 3); maps holds kBatchMaps tensor maps per
+// descriptor.
 void launch_batch_dt(BatchSolve* d, int nsolves, cudaStream_t s);
 // rows: tile height (8, 16, 32) the descriptors' work items were laid out with.  With
 // err != nullptr (every solve of the launch has maps for that height) stages 1-3 stage

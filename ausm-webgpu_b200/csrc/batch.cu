@@ -51,7 +51,7 @@ struct ausm_batch {
   ausm::BatchItem* d_items = nullptr;
   int item_cap = 0;
   int* d_steps = nullptr;  // steps taken since the item table was uploaded (d_err + 1)
-  CUtensorMap* d_maps = nullptr;  // 8 per descriptor (halo[3], plain[3], mi, mj) when tma
+  CUtensorMap* d_maps = nullptr;  // kBatchMaps per descriptor when tma
   bool tma = false;               // every member has tensor maps: stages load tiles by TMA
   int rows = 16;                  // tile height of the work list
   int tuned_rows = 0;             // height chosen by the last tuning run (0: none yet)
@@ -122,7 +122,9 @@ BatchSolve describe(const ausm_solver* h, int tile0, int chunk0, const CUtensorM
   return d;
 }
 
-const CUtensorMap* maps_of(const ausm_batch* b, int k) { return b->tma ? b->d_maps + 8 * (size_t)k : nullptr; }
+const CUtensorMap* maps_of(const ausm_batch* b, int k) {
+  return b->tma ? b->d_maps + ausm::kBatchMaps * (size_t)k : nullptr;
+}
 
 // Grows the per-member and per-tile device arrays (dropping graphs that point at them).
 int ensure_capacity(ausm_batch* b) {
@@ -140,7 +142,7 @@ int ensure_capacity(ausm_batch* b) {
     b->d_solves = nullptr; b->d_maps = nullptr; b->d_out = nullptr; b->d_l2 = nullptr; b->h_out = nullptr; b->h_l2 = nullptr;
     b->cap = 0;
     BCU(b, cudaMalloc((void**)&b->d_solves, cap * sizeof(BatchSolve)));
-    BCU(b, cudaMalloc((void**)&b->d_maps, cap * 8 * sizeof(CUtensorMap)));
+    BCU(b, cudaMalloc((void**)&b->d_maps, cap * ausm::kBatchMaps * sizeof(CUtensorMap)));
     BCU(b, cudaMalloc((void**)&b->d_out, cap * 2 * sizeof(float)));
     BCU(b, cudaMalloc((void**)&b->d_l2, cap * sizeof(double)));
     BCU(b, cudaMallocHost((void**)&b->h_out, (cap * 2 + 1) * sizeof(float)));  // + the error flag
@@ -197,7 +199,7 @@ void relayout(ausm_batch* b) {
     if (b->groups.empty() || b->groups.back().scheme != h->p.scheme) b->groups.push_back({h->p.scheme, s, s, t, t});
     b->mirror.push_back(describe(h, t, chunks, maps_of(b, s)));
     const int tx = (h->M + kTX - 1) / kTX, tiles = tx * ((h->N + rows - 1) / rows);
-    for (int k = 0; k < tiles; k++) b->items.push_back({s, 0, k % tx, k / tx});
+    for (int k = 0; k < tiles; k++) b->items.push_back({s, 0, (k % tx) | (k / tx) << 16, h->M});
     t += tiles;
     chunks += (int)(((size_t)h->M * h->N + kNormChunk - 1) / kNormChunk);
     b->groups.back().s_hi = s + 1;
@@ -229,13 +231,14 @@ int sync_descriptors(ausm_batch* b) {
                            cudaMemcpyHostToDevice, b->st));
     if (b->tma) {  // each member's maps, in work-list order
       std::vector<CUtensorMap> maps;
-      maps.reserve(8 * b->members.size());
+      maps.reserve(ausm::kBatchMaps * b->members.size());
       for (int k : b->order) {
         const ausm::TmaMaps& t = b->members[k]->tma[ausm::tile_index(b->rows)];
         for (int q = 0; q < 3; q++) maps.push_back(t.halo[q]);
         for (int q = 0; q < 3; q++) maps.push_back(t.plain[q]);
         maps.push_back(t.mi);
         maps.push_back(t.mj);
+        for (int q = 0; q < 3; q++) maps.push_back(t.wrap[q]);
       }
       BCU(b, cudaMemcpyAsync(b->d_maps, maps.data(), maps.size() * sizeof(CUtensorMap), cudaMemcpyHostToDevice,
                              b->st));

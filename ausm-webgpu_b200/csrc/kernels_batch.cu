@@ -36,13 +36,13 @@ template <int TY> struct LdgSmem {
 // current buffer and its tile origin.  The buffer index is the solve's rotation when
 // the table was written plus the steps the batch has taken since (*steps) plus rot.
 struct ItemTile {
-  int s, a, i0, j0;
+  int s, a, i0, j0, M;
 };
 template <int TY>
 __device__ __forceinline__ ItemTile item_tile(const BatchItem* __restrict__ items, const int* __restrict__ steps,
                                               int item, int rot) {
   const BatchItem it = items[item];
-  return {it.solve, (it.cur + *steps + rot) % 3, (int)it.ti * TX, (int)it.tj * TY};
+  return {it.solve, (it.cur + *steps + rot) % 3, (it.tile & 0xffff) * TX, (it.tile >> 16) * TY, it.M};
 }
 
 // One CTA per work item of one scheme group; per-thread loads.
@@ -76,7 +76,8 @@ __global__ void __launch_bounds__(Geo<TY>::NT, Geo<TY>::MIN_BLOCKS)
 }
 
 // TMA-staged form (stages 1-3): the tile's boxes come through the solve's own tensor
-// maps (in global memory, 8 per solve in descriptor order, for this tile height).
+// maps (in global memory, kBatchMaps per solve in descriptor order, for this tile
+// height).
 template <int SCHEME, int STAGE, bool EMIT, int TY>
 __global__ void __launch_bounds__(Geo<TY>::NT, Geo<TY>::MIN_BLOCKS)
     k_batch_stage_tma(const BatchSolve* __restrict__ solves, const BatchItem* __restrict__ items,
@@ -87,9 +88,9 @@ __global__ void __launch_bounds__(Geo<TY>::NT, Geo<TY>::MIN_BLOCKS)
   const ItemTile w0 = item_tile<TY>(items, steps, t0 + blockIdx.x, rot);
   const int a = w0.a, b = (a + 1) % 3, c3 = (a + 2) % 3;
   const int s_in = STAGE == 1 ? a : (STAGE == 2 ? b : c3);
-  const CUtensorMap* mp = maps + 8 * (size_t)w0.s;
+  const CUtensorMap* mp = maps + kBatchMaps * (size_t)w0.s;
   if (threadIdx.y * NWX + threadIdx.x == 0)
-    tile_tma_issue<STAGE, TY>(&mp[s_in], &mp[3 + a], &mp[6], &mp[7], smem, w0.i0, w0.j0);
+    tile_tma_issue<STAGE, TY>(&mp[s_in], &mp[3 + a], &mp[6], &mp[7], &mp[8 + s_in], smem, w0.i0, w0.j0, w0.M);
   const BatchSolve& d = solves[w0.s];  // read while the boxes land
   const Consts c = d.c;
   uint32_t wmax = 0u;

@@ -220,8 +220,8 @@ __global__ void __launch_bounds__(Geo<TY>::NT, Geo<TY>::MIN_BLOCKS)
   extern __shared__ __align__(128) unsigned char smem_raw[];
   unsigned char* smem = smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u);
   uint32_t wmax = 0u;
-  if (!tile_tma_body<SCHEME, STAGE, EMIT, TY>(smem, &tm.qs, &tm.qn, &tm.mi, &tm.mj, Qs, Qo, Mi, Mj, *dtp, c, M, N,
-                                              blockIdx.x * TX, blockIdx.y * TY, err, wmax))
+  if (!tile_tma_body<SCHEME, STAGE, EMIT, TY>(smem, &tm.qs, &tm.qn, &tm.mi, &tm.mj, &tm.wrap, Qs, Qo, Mi, Mj, *dtp, c,
+                                              M, N, blockIdx.x * TX, blockIdx.y * TY, err, wmax))
     return;
   if constexpr (EMIT) block_max_to(wave, wmax);
 }
@@ -303,9 +303,9 @@ void launch_fused_stage(int scheme, int stage, bool emit, const float4* Qs, cons
 
 // Tensor maps of the TMA kernels for tile height ty: state buffers as 2-D float tensors
 // of 4M x N (row pitch 16 M bytes) with the halo box 144 x (ty+4) and the Qn box
-// 128 x ty; face records Mi as 4M x N with the box 132 x ty, Mj as 4M x (N+1) with the
-// box 128 x (ty+1).  Every box's row is a multiple of 16 bytes and every x coordinate a
-// multiple of 4 floats (16 bytes).
+// 128 x ty and the seam box 8 x (ty+4); face records Mi as 4M x N with the box
+// 132 x ty, Mj as 4M x (N+1) with the box 128 x (ty+1).  Every box's row is a multiple
+// of 16 bytes and every x coordinate a multiple of 4 floats (16 bytes).
 bool encode_tma_maps(const float4* const Q[3], const float4* Mi, const float4* Mj, int M, int N, int ty,
                      TmaMaps* out) {
   out->ok = false;
@@ -336,6 +336,8 @@ bool encode_tma_maps(const float4* const Q[3], const float4* Mi, const float4* M
     if (!enc(&out->halo[b], Q[b], 4ull * M, N, 16ull * M, 4 * (TX + 4), bty + 4)) return false;
     if (!enc(&out->plain[b], Q[b], 4ull * M, N, 16ull * M, 4 * TX, bty)) return false;
   }
+  for (int b = 0; b < 3; b++)
+    if (!enc(&out->wrap[b], Q[b], 4ull * M, N, 16ull * M, 8, bty + 4)) return false;
   if (!enc(&out->mi, Mi, 4ull * M, N, 16ull * M, 4 * (TX + 1), bty)) return false;
   if (!enc(&out->mj, Mj, 4ull * M, N + 1, 16ull * M, 4 * TX, bty + 1)) return false;
   out->ok = true;

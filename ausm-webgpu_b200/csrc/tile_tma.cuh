@@ -1,9 +1,9 @@
 // TMA staging of one stage tile (one tile per CTA): the state box with its 2-cell halo
-// (36 x (TY+4) float4), the face-record boxes (33 x TY i-faces, 32 x (TY+1) j-faces)
-// and, for stages 2 and 3, the Qn box (32 x TY) land in shared memory by four
-// cp.async.bulk.tensor copies (no multicast) completing on three mbarriers; the threads
-// then fill the seam columns and ghost rows the boxes cannot hold and run the tile
-// compute of stage_tile.cuh.  Used by the single-solve kernel (tensor maps as a kernel
+// (36 x (TY+4) float4), the face-record boxes (33 x TY i-faces, 32 x (TY+1) j-faces),
+// for stages 2 and 3 the Qn box (32 x TY) and, for a tile at the seam, the two columns
+// its halo wraps to (2 x (TY+4)) land in shared memory by cp.async.bulk.tensor copies
+// (no multicast) completing on three mbarriers; the threads then fill the ghost rows
+// the boxes cannot hold and run the tile compute of stage_tile.cuh.  Used by the single-solve kernel (tensor maps as a kernel
 // parameter) and the batched kernel (per-solve tensor maps in global memory, written
 // by the host before the launch).
 #pragma once
@@ -22,25 +22,33 @@ template <int TY> struct T1 {
   static constexpr int SI = TY * (TX + 1) * 16;        // i-face box
   static constexpr int SJ = (TY + 1) * TX * 16;        // j-face box
   static constexpr int SN = TY * TX * 16;              // Qn box
+  static constexpr int SW = (TY + 4) * 2 * 16;         // seam box
   static constexpr int OFF_I = r128(SQ), OFF_J = OFF_I + r128(SI), OFF_N = OFF_J + r128(SJ);
-  static constexpr int OFF_BAR = OFF_N + r128(SN);
+  static constexpr int OFF_W = OFF_N + r128(SN);       // left and right seam boxes
+  static constexpr int OFF_BAR = OFF_W + 2 * r128(SW);
   static constexpr int SMEM = OFF_BAR + 128 + 128;  // 3 mbarriers + alignment slack of the base
 };
 
-// Issues the tile's boxes (thread 0): the state box on barrier 0, the two face-record
-// boxes on barrier 1, Qn (stages 2, 3) on barrier 2, so each phase waits only for what
-// it reads.
+// Issues the tile's boxes (thread 0): the state box and the seam boxes on barrier 0,
+// the two face-record boxes on barrier 1, Qn (stages 2, 3) on barrier 2, so each phase
+// waits only for what it reads.  Seam boxes: a tile whose halo starts left of column 0
+// gets columns M-2, M-1 (left box), one whose halo reaches column M gets columns 0, 1
+// (right box).
 template <int STAGE, int TY>
 __device__ __forceinline__ void tile_tma_issue(const CUtensorMap* qs, const CUtensorMap* qn, const CUtensorMap* mi,
-                                               const CUtensorMap* mj, unsigned char* smem, int i0, int j0) {
+                                               const CUtensorMap* mj, const CUtensorMap* wr, unsigned char* smem,
+                                               int i0, int j0, int M) {
   using L = T1<TY>;
   uint64_t* bar = reinterpret_cast<uint64_t*>(smem + L::OFF_BAR);
+  const bool wl = i0 == 0, wrr = i0 + TX + 2 > M;
   mbar_init(&bar[0], 1);
   mbar_init(&bar[1], 1);
   mbar_init(&bar[2], 1);
   mbar_fence_init();
-  mbar_expect_tx(&bar[0], L::SQ);
+  mbar_expect_tx(&bar[0], L::SQ + (wl ? L::SW : 0) + (wrr ? L::SW : 0));
   tma_load_2d(smem, qs, 4 * (i0 - 2), j0 - 2, &bar[0]);
+  if (wl) tma_load_2d(smem + L::OFF_W, wr, 4 * (M - 2), j0 - 2, &bar[0]);
+  if (wrr) tma_load_2d(smem + L::OFF_W + r128(L::SW), wr, 0, j0 - 2, &bar[0]);
   mbar_expect_tx(&bar[1], L::SI + L::SJ);
   tma_load_2d(smem + L::OFF_I, mi, 4 * i0, j0, &bar[1]);
   tma_load_2d(smem + L::OFF_J, mj, 4 * i0, j0, &bar[1]);
@@ -86,18 +94,22 @@ __device__ __forceinline__ bool tile_tma_compute(unsigned char* smem, const floa
   float4(*Ti)[TX + 1] = reinterpret_cast<float4(*)[TX + 1]>(smem + L::OFF_I);
   float4(*Tj)[TX] = reinterpret_cast<float4(*)[TX]>(smem + L::OFF_J);
   float4(*SN)[TX] = reinterpret_cast<float4(*)[TX]>(smem + L::OFF_N);
+  float4(*WL)[2] = reinterpret_cast<float4(*)[2]>(smem + L::OFF_W);             // columns M-2, M-1
+  float4(*WR)[2] = reinterpret_cast<float4(*)[2]>(smem + L::OFF_W + r128(L::SW));  // columns 0, 1
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * NWX + tx;
 
-  // fill seam columns and ghost rows the state box could not hold, keep the owned
-  // conserved states, convert to primitives in place (the face records are landing)
+  // take the seam columns from the seam boxes, keep the owned conserved states, convert
+  // to primitives in place (the face records are landing); ghost rows are filled once
+  // the records have landed (below)
   auto stage_entry = [&](int pr, int pc) {
     float4 q;
     if constexpr (INNER) {
       q = P[pr][pc];
     } else {
       const int ig = i0 - 2 + pc, j = j0 - 2 + pr;
-      if (j >= 0 && j < N) q = (ig >= 0 && ig < M) ? P[pr][pc] : __ldg(&Qs[(size_t)j * M + wrap_i(ig, M)]);
-      else q = tile_cell(Qs, Mj, c, M, N, wrap_i(ig, M), j);
+      const float4 none = make_float4(1.0f, 0.0f, 0.0f, 1.0f);  // never read by a face of the grid
+      if (j >= 0 && j < N) q = ig < 0 ? WL[pr][ig + 2] : (ig < M ? P[pr][pc] : (ig < M + 2 ? WR[pr][ig - M] : none));
+      else q = none;  // a ghost row (set below) or beyond it
     }
     P[pr][pc] = to_prim<true>(q, c.gm1);
     return q;
@@ -114,11 +126,33 @@ __device__ __forceinline__ bool tile_tma_compute(unsigned char* smem, const floa
     }
   }
   if (!tile_tma_wait<STAGE, TY>(smem, 1, tid, err)) return false;  // also orders the P writes
-  if (!INNER && i0 + TX >= M) {  // uniform per CTA: the face column past the seam (zero-filled by the box)
-    if (tx == 0)
+  if constexpr (!INNER) {
+    // ghost rows (boundary pass ausm.js:34-120; loadState's clamp ausm.js:141 maps rows
+    // -2 and -1 to the wall ghost), each computed once per column by the thread that
+    // holds the adjacent interior cell, with the face normal from the landed records
+    const bool wall = j0 == 0, far = j0 + TY + 2 > N, seam = i0 + TX >= M;  // uniform per CTA
+    const int i = i0 + tx;
+    if (wall && ty == 0 && i < M) {
+      const float4 g = to_prim<true>(wall_ghost_n<true>(qa, Tj[0][tx].x, Tj[0][tx].y), c.gm1);
+      P[0][tx + 2] = g;
+      P[1][tx + 2] = g;
+    }
+    if (far && i < M) {
+      const int r = N - 1 - j0;  // tile row of the last interior row; r == TY: the halo row above
+      const bool mine = r < TY && ty == (r < NWY ? r : r - NWY);
+      if (mine || (r == TY && ty == 0)) {
+        const float4 s = r < TY ? (r < NWY ? qa : qb) : __ldg(&Qs[(size_t)(N - 1) * M + i]);
+        const float4 f = N - j0 <= TY ? Tj[N - j0][tx] : __ldg(&Mj[(size_t)N * M + i]);
+        float4 g1, g2;
+        far_ghosts_n<true>(s, f.x, f.y, c, g1, g2);
+        P[r + 3][tx + 2] = to_prim<true>(g1, c.gm1);
+        if (r + 4 <= TY + 3) P[r + 4][tx + 2] = to_prim<true>(g2, c.gm1);
+      }
+    }
+    if (seam && tx == 0)  // the face column past the seam (zero-filled by the box)
       for (int r = ty; r < TY; r += NWY)
         if (j0 + r < N) Ti[r][M - i0] = __ldg(&Mi[(size_t)(j0 + r) * M]);
-    __syncthreads();
+    if (wall || far || seam) __syncthreads();
   }
   const FaceW w = own_weights<TY>(Ti, Tj, tx, ty);
   faces_phase<SCHEME, TY, INNER>(P, Ti, Tj, c, i0, j0, M, N, tx, ty);
@@ -150,12 +184,12 @@ __device__ __forceinline__ bool tile_tma_run(unsigned char* smem, const float4* 
 // The whole stage of tile (i0, j0): issue, then tile_tma_run.
 template <int SCHEME, int STAGE, bool EMIT, int TY>
 __device__ __forceinline__ bool tile_tma_body(unsigned char* smem, const CUtensorMap* qs, const CUtensorMap* qn,
-                                              const CUtensorMap* mi, const CUtensorMap* mj,
+                                              const CUtensorMap* mi, const CUtensorMap* mj, const CUtensorMap* wr,
                                               const float4* __restrict__ Qs, float4* __restrict__ Qo,
                                               const float4* __restrict__ Mi, const float4* __restrict__ Mj, float dt,
                                               const Consts& c, int M, int N, int i0, int j0, int* err,
                                               uint32_t& wmax) {
-  if (threadIdx.y * NWX + threadIdx.x == 0) tile_tma_issue<STAGE, TY>(qs, qn, mi, mj, smem, i0, j0);
+  if (threadIdx.y * NWX + threadIdx.x == 0) tile_tma_issue<STAGE, TY>(qs, qn, mi, mj, wr, smem, i0, j0, M);
   return tile_tma_run<SCHEME, STAGE, EMIT, TY>(smem, Qs, Qo, Mi, Mj, dt, c, M, N, i0, j0, err, wmax);
 }
 
