@@ -5,6 +5,7 @@
 #include <stdint.h>
 
 #include <algorithm>
+#include <cstdlib>
 
 #include "physics.cuh"
 #include "physics_exact.cuh"
@@ -15,6 +16,32 @@ namespace ausm {
 // Block-wide max of non-negative float bit patterns (u32 order == float order for
 // x >= 0; NaN bit patterns compare above +inf, so a NaN wave speed propagates and the
 // host reports divergence).  One atomicMax per block into *dst.  All threads call it.
+// Launch with programmatic stream serialization: the kernel may start while its
+// stream predecessor is still running and waits for it with grid_dep_wait (tma.cuh)
+// before reading anything that kernel writes.  AUSM_PDL=0 launches plainly (A/B
+// timing).
+inline bool pdl_enabled() {
+  static const bool on = [] {
+    const char* e = std::getenv("AUSM_PDL");
+    return !(e && e[0] == '0');
+  }();
+  return on;
+}
+template <class... KArgs, class... Args>
+cudaError_t launch_pdl(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, Args&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = pdl_enabled() ? 1 : 0;
+  return cudaLaunchKernelEx(&cfg, kern, static_cast<Args&&>(args)...);
+}
+
 __device__ __forceinline__ void block_max_to(uint32_t* dst, uint32_t v) {
   __shared__ uint32_t warp_max[32];
   v = __reduce_max_sync(0xffffffffu, v);

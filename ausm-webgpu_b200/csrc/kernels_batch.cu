@@ -57,6 +57,8 @@ __global__ void __launch_bounds__(Geo<TY>::NT, Geo<TY>::MIN_BLOCKS)
   float4(*Tj)[TX] = reinterpret_cast<float4(*)[TX]>(smem_ldg + LdgSmem<TY>::OFF_J);
   const int tx = threadIdx.x, ty = threadIdx.y;
   const ItemTile w0 = item_tile<TY>(items, steps, t0 + blockIdx.x, rot);
+  grid_dep_wait();  // the previous stage (and the dt of this step) complete
+  grid_dep_launch();
   const BatchSolve& d = solves[w0.s];
   const Consts c = d.c;
   const int M = d.M, N = d.N, i0 = w0.i0, j0 = w0.j0;
@@ -89,8 +91,11 @@ __global__ void __launch_bounds__(Geo<TY>::NT, Geo<TY>::MIN_BLOCKS)
   const int a = w0.a, b = (a + 1) % 3, c3 = (a + 2) % 3;
   const int s_in = STAGE == 1 ? a : (STAGE == 2 ? b : c3);
   const CUtensorMap* mp = maps + kBatchMaps * (size_t)w0.s;
-  if (threadIdx.y * NWX + threadIdx.x == 0)
-    tile_tma_issue<STAGE, TY>(&mp[s_in], &mp[3 + a], &mp[6], &mp[7], &mp[8 + s_in], smem, w0.i0, w0.j0, w0.M);
+  const bool lead = threadIdx.y * NWX + threadIdx.x == 0;
+  if (lead) tile_tma_issue_records<TY>(&mp[6], &mp[7], smem, w0.i0, w0.j0);
+  grid_dep_wait();  // the previous stage (and the dt of this step) complete
+  grid_dep_launch();
+  if (lead) tile_tma_issue_state<STAGE, TY>(&mp[s_in], &mp[3 + a], &mp[8 + s_in], smem, w0.i0, w0.j0, w0.M);
   const BatchSolve& d = solves[w0.s];  // read while the boxes land
   const Consts c = d.c;
   uint32_t wmax = 0u;
@@ -199,7 +204,8 @@ void launch_b(const BatchSolve* d, const BatchItem* items, const int* steps, con
                              T1<TY>::SMEM);
         attr = true;
       }
-      k_batch_stage_tma<SC, ST, E, TY><<<t_hi - t_lo, block, T1<TY>::SMEM, s>>>(d, items, steps, maps, t_lo, rot, err);
+      launch_pdl(k_batch_stage_tma<SC, ST, E, TY>, dim3(t_hi - t_lo), block, T1<TY>::SMEM, s, d, items, steps, maps,
+                 t_lo, rot, err);
       return;
     }
   }
@@ -211,7 +217,8 @@ void launch_b(const BatchSolve* d, const BatchItem* items, const int* steps, con
                            LdgSmem<TY>::BYTES);
       attr = true;
     }
-    k_batch_stage<SC, ST, E, TY><<<t_hi - t_lo, block, LdgSmem<TY>::BYTES, s>>>(d, items, steps, t_lo, rot);
+    launch_pdl(k_batch_stage<SC, ST, E, TY>, dim3(t_hi - t_lo), block, LdgSmem<TY>::BYTES, s, d, items, steps, t_lo,
+               rot);
   }
 }
 template <int SC, int TY>

@@ -238,7 +238,7 @@ void launch_tile(const float4* Qs, float4* Qo, const float4* Mi, const float4* M
     attr = true;
   }
   const dim3 grid((M + TX - 1) / TX, (N + TY - 1) / TY);
-  kern<<<grid, dim3(NWX, Geo<TY>::NWY), T1<TY>::SMEM, s>>>(*tm, Qs, Qo, Mi, Mj, dt, wave, err, c, M, N);
+  launch_pdl(kern, grid, dim3(NWX, Geo<TY>::NWY), T1<TY>::SMEM, s, *tm, Qs, Qo, Mi, Mj, dt, wave, err, c, M, N);
 }
 
 template <int S, int ST, bool E>

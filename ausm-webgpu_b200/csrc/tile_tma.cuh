@@ -29,29 +29,37 @@ template <int TY> struct T1 {
   static constexpr int SMEM = OFF_BAR + 128 + 128;  // 3 mbarriers + alignment slack of the base
 };
 
-// Issues the tile's boxes (thread 0): the state box and the seam boxes on barrier 0,
-// the two face-record boxes on barrier 1, Qn (stages 2, 3) on barrier 2, so each phase
-// waits only for what it reads.  Seam boxes: a tile whose halo starts left of column 0
-// gets columns M-2, M-1 (left box), one whose halo reaches column M gets columns 0, 1
-// (right box).
-template <int STAGE, int TY>
-__device__ __forceinline__ void tile_tma_issue(const CUtensorMap* qs, const CUtensorMap* qn, const CUtensorMap* mi,
-                                               const CUtensorMap* mj, const CUtensorMap* wr, unsigned char* smem,
-                                               int i0, int j0, int M) {
+// The tile's loads, issued by thread 0 in two parts: first the barriers and the
+// face-record boxes (barrier 1; the records never change, so this part may run before
+// the previous stage has finished), then, once the previous stage's writes are
+// visible (tile_tma_issue's caller waits for them), the state box and the seam boxes
+// (barrier 0) and Qn (stages 2, 3; barrier 2), so each phase waits only for what it
+// reads.  Seam boxes: a tile whose halo starts left of column 0 gets columns M-2, M-1
+// (left box), one whose halo reaches column M gets columns 0, 1 (right box).
+template <int TY>
+__device__ __forceinline__ void tile_tma_issue_records(const CUtensorMap* mi, const CUtensorMap* mj,
+                                                       unsigned char* smem, int i0, int j0) {
   using L = T1<TY>;
   uint64_t* bar = reinterpret_cast<uint64_t*>(smem + L::OFF_BAR);
-  const bool wl = i0 == 0, wrr = i0 + TX + 2 > M;
   mbar_init(&bar[0], 1);
   mbar_init(&bar[1], 1);
   mbar_init(&bar[2], 1);
   mbar_fence_init();
+  mbar_expect_tx(&bar[1], L::SI + L::SJ);
+  tma_load_2d(smem + L::OFF_I, mi, 4 * i0, j0, &bar[1]);
+  tma_load_2d(smem + L::OFF_J, mj, 4 * i0, j0, &bar[1]);
+}
+template <int STAGE, int TY>
+__device__ __forceinline__ void tile_tma_issue_state(const CUtensorMap* qs, const CUtensorMap* qn,
+                                                     const CUtensorMap* wr, unsigned char* smem, int i0, int j0,
+                                                     int M) {
+  using L = T1<TY>;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem + L::OFF_BAR);
+  const bool wl = i0 == 0, wrr = i0 + TX + 2 > M;
   mbar_expect_tx(&bar[0], L::SQ + (wl ? L::SW : 0) + (wrr ? L::SW : 0));
   tma_load_2d(smem, qs, 4 * (i0 - 2), j0 - 2, &bar[0]);
   if (wl) tma_load_2d(smem + L::OFF_W, wr, 4 * (M - 2), j0 - 2, &bar[0]);
   if (wrr) tma_load_2d(smem + L::OFF_W + r128(L::SW), wr, 0, j0 - 2, &bar[0]);
-  mbar_expect_tx(&bar[1], L::SI + L::SJ);
-  tma_load_2d(smem + L::OFF_I, mi, 4 * i0, j0, &bar[1]);
-  tma_load_2d(smem + L::OFF_J, mj, 4 * i0, j0, &bar[1]);
   if constexpr (STAGE >= 2) {
     mbar_expect_tx(&bar[2], L::SN);
     tma_load_2d(smem + L::OFF_N, qn, 4 * i0, j0, &bar[2]);
@@ -166,7 +174,7 @@ __device__ __forceinline__ bool tile_tma_compute(unsigned char* smem, const floa
   return true;
 }
 
-// The stage of tile (i0, j0) after thread 0 has issued its loads (tile_tma_issue);
+// The stage of tile (i0, j0) after thread 0 has issued its loads;
 // wmax gets the tile's max wave-speed bits (EMIT).  Returns false (nothing written)
 // when one of the tile's loads timed out.
 template <int SCHEME, int STAGE, bool EMIT, int TY>
@@ -181,7 +189,8 @@ __device__ __forceinline__ bool tile_tma_run(unsigned char* smem, const float4* 
   return tile_tma_compute<SCHEME, STAGE, EMIT, TY, false>(smem, Qs, Qo, Mi, Mj, dt, c, M, N, i0, j0, err, wmax);
 }
 
-// The whole stage of tile (i0, j0): issue, then tile_tma_run.
+// The whole stage of tile (i0, j0): the record loads, the wait for the previous stage
+// (programmatic dependent launch), the state loads, then tile_tma_run.
 template <int SCHEME, int STAGE, bool EMIT, int TY>
 __device__ __forceinline__ bool tile_tma_body(unsigned char* smem, const CUtensorMap* qs, const CUtensorMap* qn,
                                               const CUtensorMap* mi, const CUtensorMap* mj, const CUtensorMap* wr,
@@ -189,7 +198,11 @@ __device__ __forceinline__ bool tile_tma_body(unsigned char* smem, const CUtenso
                                               const float4* __restrict__ Mi, const float4* __restrict__ Mj, float dt,
                                               const Consts& c, int M, int N, int i0, int j0, int* err,
                                               uint32_t& wmax) {
-  if (threadIdx.y * NWX + threadIdx.x == 0) tile_tma_issue<STAGE, TY>(qs, qn, mi, mj, wr, smem, i0, j0, M);
+  const bool lead = threadIdx.y * NWX + threadIdx.x == 0;
+  if (lead) tile_tma_issue_records<TY>(mi, mj, smem, i0, j0);
+  grid_dep_wait();
+  grid_dep_launch();
+  if (lead) tile_tma_issue_state<STAGE, TY>(qs, qn, wr, smem, i0, j0, M);
   return tile_tma_run<SCHEME, STAGE, EMIT, TY>(smem, Qs, Qo, Mi, Mj, dt, c, M, N, i0, j0, err, wmax);
 }
 

@@ -31,6 +31,13 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, i
       "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
       : "memory");
 }
+// Programmatic dependent launch: a kernel launched with the programmatic-serialization
+// attribute may start while the previous kernel in its stream is still running.  It
+// reads nothing that kernel (or a later-finishing one before it) writes until
+// grid_dep_wait() returns; grid_dep_launch() lets the next such kernel start early.
+// Both are no-ops for a kernel launched without the attribute.
+__device__ __forceinline__ void grid_dep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void grid_dep_launch() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
   uint32_t ok;
   asm volatile(
