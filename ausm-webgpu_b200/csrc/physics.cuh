@@ -326,9 +326,10 @@ __device__ __forceinline__ float4 face_flux_len(float4 L2, float4 L, float4 R, f
     const float Mbar2 = 0.5f * fmaf(MR, MR, ML * ML);
     const float Mo2 = fminf(1.0f, fmaxf(Mbar2, Minf2));
     const float fa = Mo2 * (2.0f - Mo2);
-    const float Mp1L = ML + 1.0f, Mp1R = MR + 1.0f, Mm1L = ML - 1.0f, Mm1R = MR - 1.0f;
-    const float M2pL = 0.25f * Mp1L * Mp1L, M2pR = 0.25f * Mp1R * Mp1R;
-    const float M2mL = -0.25f * Mm1L * Mm1L, M2mR = -0.25f * Mm1R * Mm1R;
+    // M2+(M) = (M+1)^2/4 = ((M+1)/2)^2, M2-(M) = -((M-1)/2)^2
+    const float hpL = fmaf(0.5f, ML, 0.5f), hpR = fmaf(0.5f, MR, 0.5f);
+    const float hmL = fmaf(0.5f, ML, -0.5f), hmR = fmaf(0.5f, MR, -0.5f);
+    const float M2pL = hpL * hpL, M2pR = hpR * hpR, M2mL = -(hmL * hmL), M2mR = -(hmR * hmR);
     const bool supL = 1.0f <= fabsf(ML), supR = 1.0f <= fabsf(MR);
     const float M4L = supL ? fmaxf(0.0f, ML) : M2pL * fmaf(2.0f, M2mL, 1.0f);
     const float M4R = supR ? fminf(0.0f, MR) : M2mR * fmaf(-2.0f, M2pR, 1.0f);
@@ -340,7 +341,7 @@ __device__ __forceinline__ float4 face_flux_len(float4 L2, float4 L, float4 R, f
     const float alpha4 = 0.75f * fmaf(5.0f * fa, fa, -4.0f);
     const float P5L = supL ? (0.0f <= ML ? 1.0f : 0.0f) : M2pL * fmaf(alpha4 * ML, M2mL, 2.0f - ML);
     const float P5R = supR ? (0.0f <= -MR ? 1.0f : 0.0f) : M2mR * fmaf(-alpha4 * MR, M2pR, -2.0f - MR);
-    const float P = fmaf(P5L, pL, P5R * pR) - c.Ku * P5L * P5R * (rhoL + rhoR) * fa * a * (uR - uL);
+    const float P = fmaf(-c.Ku * P5L * P5R * (rhoL + rhoR) * fa * a, uR - uL, fmaf(P5L, pL, P5R * pR));
     const float mdot = a * Mi * (Mi > 0.0f ? rhoL : rhoR);
     const bool left = mdot > 0.0f;
     const float len = hl + hl;

@@ -7,8 +7,8 @@ at 40 chords, geometric radial stretching with a first cell of 1e-3 chord, M = 6
 AoA = 4 deg, SLAU2 + MUSCL, TVD-RK3, CFL 0.5, FP32 state, uniform freestream start
 (the large precision-study configuration).  Synthetic: the grid and flow are generated
 here, there is no dataset.  One timed step = one TVD-RK3 step (three fused stage
-launches) of the whole grid; the 201 MB state and 100 MB vertex arrays are larger than
-the 126 MB L2, so every step streams them from HBM.
+launches) of the whole grid; the 201 MB state buffers and 403 MB of face records are
+larger than the 126 MB L2, so every step streams them from HBM.
 
 Multi-GPU (torchrun): every rank advances its own replica of the grid (solves are
 independent; there is no data-path collective), value = all ranks' cell-updates / the
