@@ -125,7 +125,7 @@ int tuned_tile_rows(ausm_solver* h, bool force, int* rows) {
       if (!tm.ok) continue;
       const TmaMapsLaunch t = {tm.halo[a], tm.plain[a], tm.mi, tm.mj, tm.wrap[a]};
       auto launch = [&] {
-        launch_fused_stage(h->p.scheme, 1, false, h->Q[a], nullptr, h->Q[b], h->Mi, h->Mj, h->dt, h->wave, h->c,
+        launch_fused_stage(h->p.scheme, 1, false, h->Q[a], nullptr, h->Q[b], h->Mi, h->Mj, h->dt, h->wave, 0, h->c,
                            h->M, h->N, &t, kTileHeights[k], h->err_flag, h->st);
       };
       launch();  // warm-up (first-launch attribute set-up, caches)
@@ -785,9 +785,11 @@ int ausm_step(ausm_solver* h, int n, float* dt_out) {
     }
     return AUSM_OK;
   }
-  launch_dt(h->wave, h->dt, h->c.maxdt, h->c.cfl, s);
+  if (n == 0 || h->engine != AUSM_ENGINE_FUSED) launch_dt(h->wave, h->dt, h->c.maxdt, h->c.cfl, s);
   if (n > 0) {
-    CU(h, cudaMemsetAsync(h->wave, 0, sizeof(uint32_t), s));
+    // fused: the first step's stage 1 computes dt from *wave and its stage 2 clears
+    // *wave (dt_mode 1, 2), so a step is three launches
+    if (h->engine != AUSM_ENGINE_FUSED) CU(h, cudaMemsetAsync(h->wave, 0, sizeof(uint32_t), s));
     if (h->engine == AUSM_ENGINE_FUSED) {
       int rows = 16;
       if ((rc = tuned_tile_rows(h, false, &rows))) return rc;
@@ -802,12 +804,12 @@ int ausm_step(ausm_solver* h, int n, float* dt_out) {
           t3 = {tm.halo[c3], tm.plain[a], tm.mi, tm.mj, tm.wrap[c3]};
           p1 = &t1; p2 = &t2; p3 = &t3;
         }
-        launch_fused_stage(sch, 1, false, h->Q[a], nullptr, h->Q[b], h->Mi, h->Mj, h->dt, h->wave, h->c, M, N, p1,
-                           rows, h->err_flag, s);
-        launch_fused_stage(sch, 2, false, h->Q[b], h->Q[a], h->Q[c3], h->Mi, h->Mj, h->dt, h->wave, h->c, M, N, p2,
-                           rows, h->err_flag, s);
-        launch_fused_stage(sch, 3, k == n - 1, h->Q[c3], h->Q[a], h->Q[b], h->Mi, h->Mj, h->dt, h->wave, h->c, M, N,
-                           p3, rows, h->err_flag, s);
+        launch_fused_stage(sch, 1, false, h->Q[a], nullptr, h->Q[b], h->Mi, h->Mj, h->dt, h->wave, k == 0 ? 1 : 0,
+                           h->c, M, N, p1, rows, h->err_flag, s);
+        launch_fused_stage(sch, 2, false, h->Q[b], h->Q[a], h->Q[c3], h->Mi, h->Mj, h->dt, h->wave, k == 0 ? 2 : 0,
+                           h->c, M, N, p2, rows, h->err_flag, s);
+        launch_fused_stage(sch, 3, k == n - 1, h->Q[c3], h->Q[a], h->Q[b], h->Mi, h->Mj, h->dt, h->wave, 0, h->c, M,
+                           N, p3, rows, h->err_flag, s);
         h->cur = b;
       }
     } else {
@@ -916,8 +918,8 @@ int ausm_residual_l2(ausm_solver* h, double* l2) {
     h->f64->sumsq_rho(h->parts, h->dacc, h->st);
   } else if (h->engine == AUSM_ENGINE_FUSED) {
     float4* scratch = h->Q[(h->cur + 1) % 3];
-    launch_fused_stage(h->p.scheme, 0, false, h->Q[h->cur], nullptr, scratch, h->Mi, h->Mj, h->dt, h->wave, h->c, M, N,
-                       nullptr, 16, h->err_flag, h->st);
+    launch_fused_stage(h->p.scheme, 0, false, h->Q[h->cur], nullptr, scratch, h->Mi, h->Mj, h->dt, h->wave, 0, h->c, M,
+                       N, nullptr, 16, h->err_flag, h->st);
     R = scratch;
   } else {
     launch_ref_boundary(h->S[2], h->S[0], h->V, h->c, M, N, h->st);

@@ -100,14 +100,18 @@ constexpr int kTileHeights[3] = {8, 16, 32};
 bool encode_tma_maps(const float4* const Q[3], const float4* Mi, const float4* Mj, int M, int N, int ty,
                      TmaMaps* out);
 // stage 1..3: RK stage; stage 0: write dQ/dt of Qs to Qo.  emit (stage 3 only):
-// atomicMax the new state's wave speed bits into *wave (zeroed by the caller).  With
-// tm != nullptr the persistent TMA kernel runs and sets *err on a bounded-wait timeout.
+// atomicMax the new state's wave speed bits into *wave (cleared before, see dt_mode).
+// With tm != nullptr the TMA kernel runs and sets *err on a bounded-wait timeout.
 // Mi, Mj: the FP64-computed face records (launch_metrics_d).
 // ty: tile height of the TMA tile kernel (8, 16 or 32; tm must come from maps of that
 // height); the per-thread and persistent kernels use 16.
+// dt_mode: 0 the stage reads *dt; 1 (stage 1 of a call's first step) dt = min(maxdt,
+// cfl / *wave) is computed and stored to *dt; 2 (stage 2 of that step) *wave is
+// cleared.  The TMA tile kernel does both in the kernel; for the others a dt kernel or
+// a memset runs before the stage.
 void launch_fused_stage(int scheme, int stage, bool emit, const float4* Qs, const float4* Qn, float4* Qo,
-                        const float4* Mi, const float4* Mj, const float* dt, uint32_t* wave, const Consts& c, int M,
-                        int N, const TmaMapsLaunch* tm, int ty, int* err, cudaStream_t s);
+                        const float4* Mi, const float4* Mj, float* dt, uint32_t* wave, int dt_mode, const Consts& c,
+                        int M, int N, const TmaMapsLaunch* tm, int ty, int* err, cudaStream_t s);
 void launch_wave_interior(const float4* Q, const float4* Mj, float gamma, int M, int N, uint32_t* wave,
                           cudaStream_t s);
 

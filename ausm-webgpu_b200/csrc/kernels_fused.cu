@@ -215,13 +215,13 @@ template <int SCHEME, int STAGE, bool EMIT, int TY>
 __global__ void __launch_bounds__(Geo<TY>::NT, Geo<TY>::MIN_BLOCKS)
     k_fused_tile_tma(const __grid_constant__ TmaMapsLaunch tm, const float4* __restrict__ Qs,
                      float4* __restrict__ Qo, const float4* __restrict__ Mi, const float4* __restrict__ Mj,
-                     const float* __restrict__ dtp, uint32_t* __restrict__ wave, int* __restrict__ err,
+                     float* __restrict__ dtp, uint32_t* __restrict__ wave, const int dt_mode, int* __restrict__ err,
                      const Consts c, const int M, const int N) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   unsigned char* smem = smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u);
   uint32_t wmax = 0u;
-  if (!tile_tma_body<SCHEME, STAGE, EMIT, TY>(smem, &tm.qs, &tm.qn, &tm.mi, &tm.mj, &tm.wrap, Qs, Qo, Mi, Mj, *dtp, c,
-                                              M, N, blockIdx.x * TX, blockIdx.y * TY, err, wmax))
+  if (!tile_tma_body<SCHEME, STAGE, EMIT, TY>(smem, &tm.qs, &tm.qn, &tm.mi, &tm.mj, &tm.wrap, Qs, Qo, Mi, Mj, dtp, wave,
+                                              dt_mode, c, M, N, blockIdx.x * TX, blockIdx.y * TY, err, wmax))
     return;
   if constexpr (EMIT) block_max_to(wave, wmax);
 }
@@ -229,8 +229,8 @@ __global__ void __launch_bounds__(Geo<TY>::NT, Geo<TY>::MIN_BLOCKS)
 // ---- launchers ----
 namespace {
 template <int S, int ST, bool E, int TY>
-void launch_tile(const float4* Qs, float4* Qo, const float4* Mi, const float4* Mj, const float* dt, uint32_t* wave,
-                 const Consts& c, int M, int N, const TmaMapsLaunch* tm, int* err, cudaStream_t s) {
+void launch_tile(const float4* Qs, float4* Qo, const float4* Mi, const float4* Mj, float* dt, uint32_t* wave,
+                 int dt_mode, const Consts& c, int M, int N, const TmaMapsLaunch* tm, int* err, cudaStream_t s) {
   auto kern = k_fused_tile_tma<S, ST, E, TY>;
   static bool attr = false;
   if (!attr) {
@@ -238,23 +238,30 @@ void launch_tile(const float4* Qs, float4* Qo, const float4* Mi, const float4* M
     attr = true;
   }
   const dim3 grid((M + TX - 1) / TX, (N + TY - 1) / TY);
-  launch_pdl(kern, grid, dim3(NWX, Geo<TY>::NWY), T1<TY>::SMEM, s, *tm, Qs, Qo, Mi, Mj, dt, wave, err, c, M, N);
+  launch_pdl(kern, grid, dim3(NWX, Geo<TY>::NWY), T1<TY>::SMEM, s, *tm, Qs, Qo, Mi, Mj, dt, wave, dt_mode, err, c, M,
+             N);
+}
+
+// "AUSM_TMA_MODE=persistent" selects the persistent kernel (A/B timing)
+bool persistent_mode() {
+  static const bool persistent = [] {
+    const char* e = std::getenv("AUSM_TMA_MODE");
+    return e && std::string(e) == "persistent";
+  }();
+  return persistent;
 }
 
 template <int S, int ST, bool E>
-void launch_t(const float4* Qs, const float4* Qn, float4* Qo, const float4* Mi, const float4* Mj, const float* dt,
-              uint32_t* wave, const Consts& c, int M, int N, const TmaMapsLaunch* tm, int ty, int* err,
+void launch_t(const float4* Qs, const float4* Qn, float4* Qo, const float4* Mi, const float4* Mj, float* dt,
+              uint32_t* wave, int dt_mode, const Consts& c, int M, int N, const TmaMapsLaunch* tm, int ty, int* err,
               cudaStream_t s) {
   const int tilesX = (M + TX - 1) / TX, tilesY = (N + TYD - 1) / TYD;
-  static const bool persistent = [] {
-    const char* e = std::getenv("AUSM_TMA_MODE");  // "persistent" selects the persistent kernel (A/B timing)
-    return e && std::string(e) == "persistent";
-  }();
+  const bool persistent = persistent_mode();
   if constexpr (ST != 0) {
     if (tm && !persistent) {
-      if (ty == 8) launch_tile<S, ST, E, 8>(Qs, Qo, Mi, Mj, dt, wave, c, M, N, tm, err, s);
-      else if (ty == 32) launch_tile<S, ST, E, 32>(Qs, Qo, Mi, Mj, dt, wave, c, M, N, tm, err, s);
-      else launch_tile<S, ST, E, 16>(Qs, Qo, Mi, Mj, dt, wave, c, M, N, tm, err, s);
+      if (ty == 8) launch_tile<S, ST, E, 8>(Qs, Qo, Mi, Mj, dt, wave, dt_mode, c, M, N, tm, err, s);
+      else if (ty == 32) launch_tile<S, ST, E, 32>(Qs, Qo, Mi, Mj, dt, wave, dt_mode, c, M, N, tm, err, s);
+      else launch_tile<S, ST, E, 16>(Qs, Qo, Mi, Mj, dt, wave, dt_mode, c, M, N, tm, err, s);
       return;
     }
     if (tm) {  // persistent, TY = 16
@@ -278,26 +285,31 @@ void launch_t(const float4* Qs, const float4* Qn, float4* Qo, const float4* Mi, 
 }
 template <int S>
 void launch_s(int stage, bool emit, const float4* Qs, const float4* Qn, float4* Qo, const float4* Mi,
-              const float4* Mj, const float* dt, uint32_t* wave, const Consts& c, int M, int N,
+              const float4* Mj, float* dt, uint32_t* wave, int dt_mode, const Consts& c, int M, int N,
               const TmaMapsLaunch* tm, int ty, int* err, cudaStream_t s) {
   switch (stage) {
-    case 0: launch_t<S, 0, false>(Qs, Qn, Qo, Mi, Mj, dt, wave, c, M, N, tm, ty, err, s); break;
-    case 1: launch_t<S, 1, false>(Qs, Qn, Qo, Mi, Mj, dt, wave, c, M, N, tm, ty, err, s); break;
-    case 2: launch_t<S, 2, false>(Qs, Qn, Qo, Mi, Mj, dt, wave, c, M, N, tm, ty, err, s); break;
+    case 0: launch_t<S, 0, false>(Qs, Qn, Qo, Mi, Mj, dt, wave, dt_mode, c, M, N, tm, ty, err, s); break;
+    case 1: launch_t<S, 1, false>(Qs, Qn, Qo, Mi, Mj, dt, wave, dt_mode, c, M, N, tm, ty, err, s); break;
+    case 2: launch_t<S, 2, false>(Qs, Qn, Qo, Mi, Mj, dt, wave, dt_mode, c, M, N, tm, ty, err, s); break;
     default:
-      if (emit) launch_t<S, 3, true>(Qs, Qn, Qo, Mi, Mj, dt, wave, c, M, N, tm, ty, err, s);
-      else launch_t<S, 3, false>(Qs, Qn, Qo, Mi, Mj, dt, wave, c, M, N, tm, ty, err, s);
+      if (emit) launch_t<S, 3, true>(Qs, Qn, Qo, Mi, Mj, dt, wave, dt_mode, c, M, N, tm, ty, err, s);
+      else launch_t<S, 3, false>(Qs, Qn, Qo, Mi, Mj, dt, wave, dt_mode, c, M, N, tm, ty, err, s);
   }
 }
 }  // namespace
 
 void launch_fused_stage(int scheme, int stage, bool emit, const float4* Qs, const float4* Qn, float4* Qo,
-                        const float4* Mi, const float4* Mj, const float* dt, uint32_t* wave, const Consts& c, int M,
-                        int N, const TmaMapsLaunch* tm, int ty, int* err, cudaStream_t s) {
+                        const float4* Mi, const float4* Mj, float* dt, uint32_t* wave, int dt_mode, const Consts& c,
+                        int M, int N, const TmaMapsLaunch* tm, int ty, int* err, cudaStream_t s) {
+  if (dt_mode != 0 && !(tm && stage != 0 && !persistent_mode())) {  // kernels without the in-kernel time step
+    if (dt_mode == 1) launch_dt(wave, dt, c.maxdt, c.cfl, s);
+    else cudaMemsetAsync(wave, 0, sizeof(uint32_t), s);
+    dt_mode = 0;
+  }
   switch (scheme) {
-    case 0: launch_s<0>(stage, emit, Qs, Qn, Qo, Mi, Mj, dt, wave, c, M, N, tm, ty, err, s); break;
-    case 1: launch_s<1>(stage, emit, Qs, Qn, Qo, Mi, Mj, dt, wave, c, M, N, tm, ty, err, s); break;
-    default: launch_s<2>(stage, emit, Qs, Qn, Qo, Mi, Mj, dt, wave, c, M, N, tm, ty, err, s); break;
+    case 0: launch_s<0>(stage, emit, Qs, Qn, Qo, Mi, Mj, dt, wave, dt_mode, c, M, N, tm, ty, err, s); break;
+    case 1: launch_s<1>(stage, emit, Qs, Qn, Qo, Mi, Mj, dt, wave, dt_mode, c, M, N, tm, ty, err, s); break;
+    default: launch_s<2>(stage, emit, Qs, Qn, Qo, Mi, Mj, dt, wave, dt_mode, c, M, N, tm, ty, err, s); break;
   }
 }
 

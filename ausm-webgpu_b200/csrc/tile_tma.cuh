@@ -189,20 +189,40 @@ __device__ __forceinline__ bool tile_tma_run(unsigned char* smem, const float4* 
   return tile_tma_compute<SCHEME, STAGE, EMIT, TY, false>(smem, Qs, Qo, Mi, Mj, dt, c, M, N, i0, j0, err, wmax);
 }
 
+// The time step of a single-solve stage launch, read after the wait for the previous
+// stage.  mode 0: *dtp.  mode 1 (stage 1 of the first step of an ausm_step call):
+// dt = min(maxdt, cfl / max wave speed) (ausm.js:457) from the wave-speed bits the
+// previous call's last stage left, computed by every CTA alike and stored to *dtp by
+// the CTA at the origin for stages 2 and 3.  mode 2 (stage 2 of that step): *dtp, and
+// the CTA at the origin clears the wave-speed accumulator (stage 1 has read it) for
+// this call's last stage 3.
+__device__ __forceinline__ float stage_dt(float* dtp, uint32_t* wave, int mode, const Consts& c, bool lead) {
+  const bool origin = lead && blockIdx.x == 0 && blockIdx.y == 0;
+  if (mode == 1) {
+    const float dt = fminf(c.maxdt, c.cfl / __uint_as_float(*wave));
+    if (origin) *dtp = dt;
+    return dt;
+  }
+  if (mode == 2 && origin) *wave = 0u;
+  return *dtp;
+}
+
 // The whole stage of tile (i0, j0): the record loads, the wait for the previous stage
-// (programmatic dependent launch), the state loads, then tile_tma_run.
+// (programmatic dependent launch), the state loads and the time step (stage_dt), then
+// tile_tma_run.
 template <int SCHEME, int STAGE, bool EMIT, int TY>
 __device__ __forceinline__ bool tile_tma_body(unsigned char* smem, const CUtensorMap* qs, const CUtensorMap* qn,
                                               const CUtensorMap* mi, const CUtensorMap* mj, const CUtensorMap* wr,
                                               const float4* __restrict__ Qs, float4* __restrict__ Qo,
-                                              const float4* __restrict__ Mi, const float4* __restrict__ Mj, float dt,
-                                              const Consts& c, int M, int N, int i0, int j0, int* err,
-                                              uint32_t& wmax) {
+                                              const float4* __restrict__ Mi, const float4* __restrict__ Mj,
+                                              float* dtp, uint32_t* wave, int dt_mode, const Consts& c, int M, int N,
+                                              int i0, int j0, int* err, uint32_t& wmax) {
   const bool lead = threadIdx.y * NWX + threadIdx.x == 0;
   if (lead) tile_tma_issue_records<TY>(mi, mj, smem, i0, j0);
   grid_dep_wait();
   grid_dep_launch();
   if (lead) tile_tma_issue_state<STAGE, TY>(qs, qn, wr, smem, i0, j0, M);
+  const float dt = stage_dt(dtp, wave, dt_mode, c, lead);
   return tile_tma_run<SCHEME, STAGE, EMIT, TY>(smem, Qs, Qo, Mi, Mj, dt, c, M, N, i0, j0, err, wmax);
 }
 
