@@ -3,12 +3,15 @@
 // the scheme groups are independent branches (their stage chains overlap on the GPU).
 //
 // Device data: one BatchSolve descriptor per member (its buffers, constants, scheme,
-// first work item and current-buffer index).  The host keeps a mirror and re-uploads it
-// when a member's constants, scheme or state buffer index changed since the last upload
-// (a parameter change, a new state, a ramp step); the graph reads the descriptors at
-// replay time, so it stays valid until the membership changes.  The buffer rotation
-// (cur) advances on the device at the end of each step sequence and in the mirror on
-// the host, identically.
+// first work item and current-buffer index), the members' tensor maps (kBatchMaps
+// each) and the item table (one BatchItem per tile: solve, rotation at upload, tile
+// coordinates, M).  The host keeps a mirror of the descriptors and re-uploads them,
+// the item table with the members' current rotations and a zeroed step counter, when a
+// member's constants, scheme or state buffer index changed since the last upload (a
+// parameter change, a new state, a ramp step); the graph reads these at replay time,
+// so it stays valid until the membership changes.  The buffer rotation (cur) advances
+// on the device at the end of each step sequence (descriptors and step counter) and in
+// the mirror on the host, identically.
 //
 // Ordering: a member's own calls run on the batch stream while it is a member, so batch
 // steps and member calls (state read-back, forces, set_params) are ordered by the

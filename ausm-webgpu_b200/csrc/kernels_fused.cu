@@ -2,31 +2,29 @@
 // five dispatches (boundary ausm.js:23, j-flux + i-flux ausm.js:271/345, residual
 // ausm.js:402, RK stage ausm.js:441/470/501).
 //
-// Work decomposition (both kernels): a CTA of 32 x 8 threads handles a TX=32 x TY=16
-// tile of interior cells; thread (x, y) owns cells (x, y) and (x, y+8) and keeps their
-// conserved state in registers.  Per tile, shared memory holds
+// Work decomposition: a CTA of 32 x TY/2 threads handles a 32 x TY tile of interior
+// cells (TY = 8, 16 or 32, stage_tile.cuh); thread (x, y) owns cells (x, y) and
+// (x, y + TY/2) and keeps their conserved state in registers.  Per tile, shared memory
+// holds
 //   - P: primitives of the tile plus a 2-cell MUSCL halo on every side (corners
-//     unused), the periodic seam wrapped in i and the ghost rows (wall j=-1,-2, far
-//     field j=N,N+1) computed in place from the interior,
-//   - Ti/Tj: the FP64-computed face records of the tile's 33 x 16 i-faces and
-//     32 x 17 j-faces (normal, length, 1/A or the wave-speed factor), overwritten in
-//     place by the flux x length of each face, evaluated once (warp w takes face rows
-//     w and w+8 of each direction; warps 0 and 1 also the top face row and the right
-//     face column),
+//     unused), with the periodic seam wrapped in i and the ghost rows (wall j=-1,-2,
+//     far field j=N,N+1) computed from the interior,
+//   - Ti/Tj: the FP64-computed face records of the tile's 33 x TY i-faces and
+//     32 x (TY+1) j-faces (normal, half length, 1/A or the wave-speed factor),
+//     overwritten by the flux x length of each face, evaluated once,
 // and each thread then assembles the residual and the stage combination of its two
 // cells and stores the new conserved states as float4.  The last stage-3 launch of a
 // step(n) call also reduces the new state's CFL wave speed (block max, one atomicMax
-// on the float bits, as cflReductionShaderCode ausm.js:535-581).
+// on the float bits, as cflReductionShaderCode ausm.js:535-581); the first step's
+// stage 1 turns it into dt.
 //
-// k_fused_stage_tma (the default) is persistent: each CTA walks tiles
-// t = blockIdx.x, blockIdx.x + gridDim.x, ... and stages them with TMA
-// (cp.async.bulk.tensor, no multicast) into a double buffer — the next tile's state
-// box (36 x 20 cells with halo) and face-record boxes load while the current tile
-// computes, and Qn for stages 2 and 3 loads during the face phase.  Out-of-range box
-// columns (the periodic seam) and rows (ghost rows) are filled in by the threads.
-// Every mbarrier wait is bounded; on a timeout the CTA sets *err and stops.
-// k_fused_stage loads the same tile with per-thread loads (AUSM_NO_TMA=1, and the
-// residual evaluation).
+// k_fused_tile_tma (the default) stages its tile with TMA (cp.async.bulk.tensor, no
+// multicast; tile_tma.cuh), one tile per CTA, launched with programmatic dependent
+// launch.  Two alternatives are kept for A/B timing: k_fused_stage_tma, persistent
+// CTAs with double-buffered 32 x 16 tiles (AUSM_TMA_MODE=persistent), and
+// k_fused_stage, per-thread loads of 32 x 16 tiles (AUSM_NO_TMA=1; also the residual
+// evaluation, stage 0).  Every mbarrier wait is bounded; on a timeout the CTA sets
+// *err and stops.
 //
 // HBM layout: interior state float4 [N][M] (row-major, no ghost rows), face records
 // float4 Mi [N][M] and Mj [N+1][M].  Traffic per cell and stage: 16 B state in, 16 B
