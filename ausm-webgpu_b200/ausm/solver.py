@@ -222,7 +222,7 @@ class Solver:
 
 
 class Batch:
-    """Many solves stepped together: one persistent kernel launch per RK stage over the
+    """Many solves stepped together: one kernel launch per RK stage and scheme over the
     tiles of every member (no counterpart in the reference, which steps one grid).
 
     Members keep their own dt, scheme and parameters; a member's results are the same

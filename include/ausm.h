@@ -198,8 +198,9 @@ int ausm_autotune(ausm_solver* h, int force, int* rows);
 
 /* ---- batches: many solves advanced together (no counterpart in the reference) ----
  * The reference steps one grid per page.  A batch steps any number of independent
- * fused-engine solvers of any grid sizes and schemes with ONE persistent kernel launch
- * per RK stage: the work list is every member's 32 x 16 cell tiles end to end.  Each
+ * fused-engine solvers of any grid sizes and schemes with one kernel launch per RK
+ * stage and scheme: the work list is every member's 32 x TY cell tiles end to end (TY
+ * chosen by the batch's tile-height tuning), one CTA per tile.  Each
  * member keeps its own dt (from its own max wave speed, held over the n steps as
  * ausm_step does), so a member's results are the same alone or in any batch.  While a
  * solver is a member, its calls run on the batch's stream (ausm_stream returns it) and
