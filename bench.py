@@ -589,7 +589,9 @@ def main():
                            "parallelism": f"replicas{world}", "l2": ("inputs larger than L2" if cells * 16 > 126e6 else "inputs fit in L2") +
                            f" ({cells * 16 / 1e6:.0f} MB state, {cells * 32 / 1e6:.0f} MB face records)",
                            "wall_s": wall},
-                "gpu_launches": (4 if args.engine == "fused" else 17) * args.steps, "clocks": clocks, "roofline": roofline, "cpu_baseline": cpu,
+                # per step(1): fused, three stage kernels (dt is computed in stage 1); reference,
+                # 5 dispatches per stage, the dt kernel and the wave-speed reduction
+                "gpu_launches": (3 if args.engine == "fused" else 17) * args.steps, "clocks": clocks, "roofline": roofline, "cpu_baseline": cpu,
                 "e2e": e2e, "batched": batched}
         print(json.dumps(line))
     if s is not None:
