@@ -102,6 +102,7 @@ _SIGS = {
     "ausm_synchronize": [_P],
     "ausm_time_steps": [_P, C.c_int, C.c_int, C.POINTER(C.c_float)],
     "ausm_autotune": [_P, C.c_int, C.POINTER(C.c_int)],
+    "ausm_debug_set_wait_polls": [C.c_uint],
     "ausm_batch_create": [C.POINTER(C.c_void_p)],
     "ausm_batch_destroy": [_P],
     "ausm_batch_add": [_P, _P],

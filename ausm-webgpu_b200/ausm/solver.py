@@ -39,6 +39,12 @@ def device_count() -> int:
     return n.value if rc == 0 else 0
 
 
+def set_wait_polls(polls: int):
+    """Test hook: polls (0..65536, the default) of the stage kernels' first bounded wait
+    for each TMA box on the current device; 0 makes every such wait give up at once."""
+    check(lib().ausm_debug_set_wait_polls(int(polls)))
+
+
 def default_params() -> AusmParams:
     p = AusmParams()
     check(lib().ausm_default_params(C.byref(p)))

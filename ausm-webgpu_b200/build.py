@@ -28,7 +28,6 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-I", str(ROOT / "include"), "-I", str(CSRC),
           "-Xptxas", "-v", "--expt-relaxed-constexpr", "-fmad=false"]
-EXTRA = os.environ.get("AUSM_NVCC_EXTRA", "").split()  # tuning sweeps, e.g. -DAUSM_FUSED_MIN_BLOCKS=4
 
 
 def sources():
@@ -40,7 +39,7 @@ def _deps():
 
 
 def up_to_date() -> bool:
-    if not OUT.exists() or EXTRA:
+    if not OUT.exists():
         return False
     t = OUT.stat().st_mtime
     return all(p.stat().st_mtime <= t for p in _deps())
@@ -55,7 +54,7 @@ def build(force: bool = False, verbose: bool = False) -> Path:
 
     def compile_one(src: Path):
         obj = objdir / (src.stem + ".o")
-        flags = list(COMMON) + EXTRA
+        flags = list(COMMON)
         cmd = [NVCC, *ARCH, *flags, "-c", str(src), "-o", str(obj)]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:

@@ -46,6 +46,7 @@ void make_consts(ausm_solver* h) {
   c.h2k = (2.0f * g) / c.gm1;
   c.ask4 = 0.25f * c.aStarK;
   c.minfk = c.Vinf2 / c.gammaInP;
+  c.hsg = 0.5f * std::sqrt(g);
   c.muscl = p.muscl;
   h->c = c;
   // FP64 constants from the FP64 parameters, in the oracle's operation order
@@ -189,6 +190,31 @@ int use_device(ausm_solver* h) {
 }
 
 double inflow_target(const AusmParams& p) { return p.mach * std::sqrt(p.gamma * p.in_pressure / p.in_rho); }
+
+// Timeout reporting.  A TMA stage kernel whose bounded wait gave up sets *err_flag
+// (device).  Every fused step queues a copy of the flag to pinned host memory; the next
+// call that waits for the stream (this step when it returns dt, or a later state,
+// force, norm, field, wave-speed, synchronize or timing call) reads it, clears the flag
+// and returns AUSM_ERR_TIMEOUT, so no path steps past a timed-out tile unreported.
+int queue_err_read(ausm_solver* h) {
+  CU(h, cudaMemcpyAsync(h->h_wave + 2, h->err_flag, sizeof(int), cudaMemcpyDeviceToHost, h->st));
+  h->err_read_queued = true;
+  return AUSM_OK;
+}
+// After the stream has been synchronised.
+int take_timeout(ausm_solver* h) {
+  if (!h->err_read_queued) return AUSM_OK;
+  h->err_read_queued = false;
+  if (h->h_wave[2] == 0) return AUSM_OK;
+  h->h_wave[2] = 0;
+  CU(h, cudaMemsetAsync(h->err_flag, 0, sizeof(int), h->st));
+  return fail(h, AUSM_ERR_TIMEOUT, "a tile load did not arrive within the bounded wait");
+}
+// Synchronises h's stream and reports a queued timeout.
+int sync_and_check(ausm_solver* h) {
+  CU(h, cudaStreamSynchronize(h->st));
+  return take_timeout(h);
+}
 
 int ensure_reference_buffers(ausm_solver* h) {
   if (h->S[0]) return AUSM_OK;
@@ -429,10 +455,8 @@ int ausm_create(int M, int N, ausm_solver** out) {
 #undef TRY
   {
     const float4* qs[3] = {h->Q[0], h->Q[1], h->Q[2]};
-    // odd M keeps the per-thread staging kernel; AUSM_NO_TMA=1 selects it for A/B timing
-    const char* no_tma = std::getenv("AUSM_NO_TMA");
-    if (!(no_tma && no_tma[0] == '1'))
-      for (int k = 0; k < 3; k++) encode_tma_maps(qs, h->Mi, h->Mj, M, N, kTileHeights[k], &h->tma[k]);
+    // a solve whose maps cannot be encoded steps with the per-thread staging kernel
+    for (int k = 0; k < 3; k++) encode_tma_maps(qs, h->Mi, h->Mj, M, N, kTileHeights[k], &h->tma[k]);
   }
   ausm_default_params(&h->p);
   h->speed_now = inflow_target(h->p);
@@ -739,8 +763,7 @@ int ausm_get_state(ausm_solver* h, float* q) {
   if (rc) return rc;
   if ((rc = state_to_staging(h))) return rc;
   CU(h, cudaMemcpyAsync(q, h->staging, (size_t)h->M * (h->N + 3) * sizeof(float4), cudaMemcpyDeviceToHost, h->st));
-  CU(h, cudaStreamSynchronize(h->st));
-  return AUSM_OK;
+  return sync_and_check(h);
 }
 
 int ausm_get_state_f64(ausm_solver* h, double* q) {
@@ -763,7 +786,12 @@ int ausm_get_state_f64(ausm_solver* h, double* q) {
   return AUSM_OK;
 }
 
-int ausm_step(ausm_solver* h, int n, float* dt_out) {
+}  // extern "C"
+
+namespace {
+// ausm_step; read_err: queue the read of the timeout flag (ausm_time_steps queues one
+// after all its repetitions instead, so that its timed steps stay back to back).
+int step_impl(ausm_solver* h, int n, float* dt_out, bool read_err) {
   NEED(h, h, AUSM_ERR_INVALID, "null handle");
   NEED(h, n >= 0, AUSM_ERR_INVALID, "n must be >= 0");
   NEED(h, h->has_grid && h->has_state, AUSM_ERR_STATE, "need a grid and a state");
@@ -834,15 +862,11 @@ int ausm_step(ausm_solver* h, int n, float* dt_out) {
   }
   CHECK_LAUNCH(h);
   ramp_after_steps(h, n);
+  if (h->engine == AUSM_ENGINE_FUSED && n > 0 && (read_err || dt_out) && (rc = queue_err_read(h))) return rc;
   if (dt_out) {
     CU(h, cudaMemcpyAsync(h->h_dt, h->dt, sizeof(float), cudaMemcpyDeviceToHost, s));
     CU(h, cudaMemcpyAsync(h->h_wave, h->wave, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
-    CU(h, cudaMemcpyAsync(h->h_wave + 2, h->err_flag, sizeof(int), cudaMemcpyDeviceToHost, s));
-    CU(h, cudaStreamSynchronize(s));
-    if (h->h_wave[2] != 0) {
-      CU(h, cudaMemsetAsync(h->err_flag, 0, sizeof(int), s));
-      return fail(h, AUSM_ERR_TIMEOUT, "a tile load did not arrive within the bounded wait");
-    }
+    if ((rc = sync_and_check(h))) return rc;
     *dt_out = h->h_dt[0];
     float w;
     std::memcpy(&w, h->h_wave, 4);
@@ -851,6 +875,11 @@ int ausm_step(ausm_solver* h, int n, float* dt_out) {
   }
   return AUSM_OK;
 }
+}  // namespace
+
+extern "C" {
+
+int ausm_step(ausm_solver* h, int n, float* dt_out) { return step_impl(h, n, dt_out, true); }
 
 int ausm_max_wave_speed(ausm_solver* h, float* out) {
   NEED(h, h, AUSM_ERR_INVALID, "null handle");
@@ -864,7 +893,7 @@ int ausm_max_wave_speed(ausm_solver* h, float* out) {
     return AUSM_OK;
   }
   CU(h, cudaMemcpyAsync(h->h_wave, h->wave, sizeof(uint32_t), cudaMemcpyDeviceToHost, h->st));
-  CU(h, cudaStreamSynchronize(h->st));
+  if ((rc = sync_and_check(h))) return rc;
   std::memcpy(out, h->h_wave, 4);
   return AUSM_OK;
 }
@@ -887,7 +916,7 @@ int ausm_forces(ausm_solver* h, double* out6, double* cp) {
   CHECK_LAUNCH(h);
   CU(h, cudaMemcpyAsync(h->h_acc, h->dacc, 2 * sizeof(double), cudaMemcpyDeviceToHost, h->st));
   if (cp) CU(h, cudaMemcpyAsync(cp, h->cp, (size_t)h->M * sizeof(double), cudaMemcpyDeviceToHost, h->st));
-  CU(h, cudaStreamSynchronize(h->st));
+  if ((rc = sync_and_check(h))) return rc;
   double Fx = h->h_acc[0], Fy = h->h_acc[1];
   double vl = std::sqrt(vx * vx + vy * vy);
   double nx = vx / vl, ny = vy / vl;
@@ -930,7 +959,7 @@ int ausm_residual_l2(ausm_solver* h, double* l2) {
   if (R) launch_sumsq_rho(R, (size_t)M * N, h->dacc, h->parts, h->st);
   CHECK_LAUNCH(h);
   CU(h, cudaMemcpyAsync(h->h_acc, h->dacc, sizeof(double), cudaMemcpyDeviceToHost, h->st));
-  CU(h, cudaStreamSynchronize(h->st));
+  if ((rc = sync_and_check(h))) return rc;
   *l2 = std::sqrt(h->h_acc[0] / ((double)M * N));
   if (!std::isfinite(*l2)) return fail(h, AUSM_ERR_DIVERGED, "residual norm is not finite: the solution diverged");
   return AUSM_OK;
@@ -957,8 +986,7 @@ int ausm_field(ausm_solver* h, int kind, float* out) {
   launch_field(q, h->V, h->c, kind, h->M, h->N, buf, h->st);
   CHECK_LAUNCH(h);
   CU(h, cudaMemcpyAsync(out, buf, (size_t)h->M * h->N * sizeof(float), cudaMemcpyDeviceToHost, h->st));
-  CU(h, cudaStreamSynchronize(h->st));
-  return AUSM_OK;
+  return sync_and_check(h);
 }
 
 int ausm_stream(ausm_solver* h, void** stream) {
@@ -970,7 +998,14 @@ int ausm_stream(ausm_solver* h, void** stream) {
 
 int ausm_synchronize(ausm_solver* h) {
   NEED(h, h, AUSM_ERR_INVALID, "null handle");
-  CU(h, cudaStreamSynchronize(h->st));
+  return sync_and_check(h);
+}
+
+int ausm_debug_set_wait_polls(unsigned polls) {
+  NEED(nullptr, polls <= 65536u, AUSM_ERR_INVALID, "polls must be in [0, 65536] (the default bound)");
+  cudaError_t e = set_wait_polls_fused(polls);
+  if (e == cudaSuccess) e = set_wait_polls_batch(polls);
+  if (e != cudaSuccess) return fail(nullptr, AUSM_ERR_CUDA, std::string("wait polls: ") + cudaGetErrorString(e));
   return AUSM_OK;
 }
 
@@ -995,13 +1030,14 @@ int ausm_time_steps(ausm_solver* h, int n, int reps, float* ms_out) {
   if (rc) return rc;
   CU(h, cudaEventRecord(h->e0, h->st));
   for (int r = 0; r < reps; r++) {
-    rc = ausm_step(h, n, nullptr);
+    rc = step_impl(h, n, nullptr, false);
     if (rc) return rc;
   }
   CU(h, cudaEventRecord(h->e1, h->st));
+  if (h->engine == AUSM_ENGINE_FUSED && (rc = queue_err_read(h))) return rc;
   CU(h, cudaEventSynchronize(h->e1));
   CU(h, cudaEventElapsedTime(ms_out, h->e0, h->e1));
-  return AUSM_OK;
+  return sync_and_check(h);
 }
 
 }  // extern "C"

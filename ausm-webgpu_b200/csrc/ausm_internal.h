@@ -104,7 +104,7 @@ bool encode_tma_maps(const float4* const Q[3], const float4* Mi, const float4* M
 // With tm != nullptr the TMA kernel runs and sets *err on a bounded-wait timeout.
 // Mi, Mj: the FP64-computed face records (launch_metrics_d).
 // ty: tile height of the TMA tile kernel (8, 16 or 32; tm must come from maps of that
-// height); the per-thread and persistent kernels use 16.
+// height); the per-thread kernel uses 16.
 // dt_mode: 0 the stage reads *dt; 1 (stage 1 of a call's first step) dt = min(maxdt,
 // cfl / *wave) is computed and stored to *dt; 2 (stage 2 of that step) *wave is
 // cleared.  The TMA tile kernel does both in the kernel; for the others a dt kernel or
@@ -114,6 +114,10 @@ void launch_fused_stage(int scheme, int stage, bool emit, const float4* Qs, cons
                         int M, int N, const TmaMapsLaunch* tm, int ty, int* err, cudaStream_t s);
 void launch_wave_interior(const float4* Q, const float4* Mj, float gamma, int M, int N, uint32_t* wave,
                           cudaStream_t s);
+// Polls of the first bounded wait of each TMA box in the single-solve and batched stage
+// kernels (ausm_debug_set_wait_polls), on the current device.
+cudaError_t set_wait_polls_fused(unsigned polls);
+cudaError_t set_wait_polls_batch(unsigned polls);
 
 // ---- batched engine (kernels_batch.cu) ----
 // One solve of a batch as the device sees it.  Its tiles are work items

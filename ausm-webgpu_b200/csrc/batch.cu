@@ -60,6 +60,8 @@ struct ausm_batch {
   int tuned_rows = 0;             // height chosen by the last tuning run (0: none yet)
   double tuned_cells = 0.0;       // the batch's cell count at that run
   int* d_err = nullptr;           // set by a TMA tile whose bounded wait gave up
+  int* h_err = nullptr;           // pinned copy of *d_err
+  bool err_read_queued = false;   // a copy of *d_err to *h_err is queued on st
   int cap = 0;  // descriptor capacity of d_solves / d_maps / d_out / d_l2
   float* d_out = nullptr;
   double* d_l2 = nullptr;
@@ -148,7 +150,7 @@ int ensure_capacity(ausm_batch* b) {
     BCU(b, cudaMalloc((void**)&b->d_maps, cap * ausm::kBatchMaps * sizeof(CUtensorMap)));
     BCU(b, cudaMalloc((void**)&b->d_out, cap * 2 * sizeof(float)));
     BCU(b, cudaMalloc((void**)&b->d_l2, cap * sizeof(double)));
-    BCU(b, cudaMallocHost((void**)&b->h_out, (cap * 2 + 1) * sizeof(float)));  // + the error flag
+    BCU(b, cudaMallocHost((void**)&b->h_out, cap * 2 * sizeof(float)));
     BCU(b, cudaMallocHost((void**)&b->h_l2, cap * sizeof(double)));
     b->cap = cap;
     b->uploaded = false;
@@ -350,6 +352,24 @@ int tune_rows(ausm_batch* b) {
   return AUSM_OK;
 }
 
+// Timeout reporting, as for one solver (api.cu): every step sequence queues a copy of
+// the batch's error flag; the next call that waits for the batch stream reads it,
+// clears the flag and returns AUSM_ERR_TIMEOUT.
+int queue_err_read(ausm_batch* b) {
+  BCU(b, cudaMemcpyAsync(b->h_err, b->d_err, sizeof(int), cudaMemcpyDeviceToHost, b->st));
+  b->err_read_queued = true;
+  return AUSM_OK;
+}
+int sync_and_check(ausm_batch* b) {
+  BCU(b, cudaStreamSynchronize(b->st));
+  if (!b->err_read_queued) return AUSM_OK;
+  b->err_read_queued = false;
+  if (*b->h_err == 0) return AUSM_OK;
+  *b->h_err = 0;
+  BCU(b, cudaMemsetAsync(b->d_err, 0, sizeof(int), b->st));
+  return bfail(b, AUSM_ERR_TIMEOUT, "a tile load did not arrive within the bounded wait");
+}
+
 int run_steps(ausm_batch* b, int n) {
   if (!b->graphs) {
     enqueue_steps(b, n);
@@ -406,6 +426,8 @@ int ausm_batch_create(ausm_batch** out) {
   e = cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming);
   if (e != cudaSuccess) return bail(e, "cudaEventCreate");
   if ((e = cudaMalloc((void**)&b->d_err, 2 * sizeof(int))) != cudaSuccess) return bail(e, "cudaMalloc");
+  if ((e = cudaMallocHost((void**)&b->h_err, sizeof(int))) != cudaSuccess) return bail(e, "cudaMallocHost");
+  *b->h_err = 0;
   if ((e = cudaMemsetAsync(b->d_err, 0, 2 * sizeof(int), b->st)) != cudaSuccess) return bail(e, "cudaMemsetAsync");
   b->d_steps = b->d_err + 1;
   *out = b;
@@ -427,6 +449,7 @@ int ausm_batch_destroy(ausm_batch* b) {
   cudaFree(b->d_part);
   if (b->h_out) cudaFreeHost(b->h_out);
   if (b->h_l2) cudaFreeHost(b->h_l2);
+  if (b->h_err) cudaFreeHost(b->h_err);
   if (b->e0) cudaEventDestroy(b->e0);
   if (b->e1) cudaEventDestroy(b->e1);
   if (b->fork) cudaEventDestroy(b->fork);
@@ -487,7 +510,11 @@ int ausm_batch_set_graphs(ausm_batch* b, int enable) {
   return AUSM_OK;
 }
 
-int ausm_batch_step(ausm_batch* b, int n, float* dt_wave) {
+}  // extern "C"
+
+namespace {
+// ausm_batch_step; read_err as in api.cu's step_impl
+int batch_step_impl(ausm_batch* b, int n, float* dt_wave, bool read_err) {
   BNEED(b, b, AUSM_ERR_INVALID, "null handle");
   BNEED(b, n >= 0, AUSM_ERR_INVALID, "n must be >= 0");
   int rc = use_dev(b);
@@ -508,16 +535,10 @@ int ausm_batch_step(ausm_batch* b, int n, float* dt_wave) {
     b->mirror[k].cur = h->cur;  // the device advanced its copy
     ausm::ramp_after_steps(h, n);
   }
+  if (b->tma && (read_err || dt_wave) && (rc = queue_err_read(b))) return rc;
   if (!dt_wave) return AUSM_OK;
   BCU(b, cudaMemcpyAsync(b->h_out, b->d_out, ns * 2 * sizeof(float), cudaMemcpyDeviceToHost, b->st));
-  BCU(b, cudaMemcpyAsync(b->h_out + 2 * b->cap, b->d_err, sizeof(int), cudaMemcpyDeviceToHost, b->st));
-  BCU(b, cudaStreamSynchronize(b->st));
-  int err_flag;
-  std::memcpy(&err_flag, b->h_out + 2 * b->cap, sizeof(int));
-  if (err_flag) {
-    BCU(b, cudaMemsetAsync(b->d_err, 0, sizeof(int), b->st));
-    return bfail(b, AUSM_ERR_TIMEOUT, "a tile load did not arrive within the bounded wait");
-  }
+  if ((rc = sync_and_check(b))) return rc;
   for (int k = 0; k < ns; k++) {
     dt_wave[2 * b->order[k]] = b->h_out[2 * k];
     dt_wave[2 * b->order[k] + 1] = b->h_out[2 * k + 1];
@@ -527,6 +548,11 @@ int ausm_batch_step(ausm_batch* b, int n, float* dt_wave) {
       return bfail(b, AUSM_ERR_DIVERGED, "member " + std::to_string(k) + ": max wave speed is not finite");
   return AUSM_OK;
 }
+}  // namespace
+
+extern "C" {
+
+int ausm_batch_step(ausm_batch* b, int n, float* dt_wave) { return batch_step_impl(b, n, dt_wave, true); }
 
 int ausm_batch_residual_l2(ausm_batch* b, double* l2) {
   BNEED(b, b && l2, AUSM_ERR_INVALID, "null argument");
@@ -542,15 +568,14 @@ int ausm_batch_residual_l2(ausm_batch* b, double* l2) {
   ausm::launch_batch_residual_norm(b->d_solves, ns, b->total_chunks, b->d_part, b->d_l2, b->st);
   BCU(b, cudaGetLastError());
   BCU(b, cudaMemcpyAsync(b->h_l2, b->d_l2, ns * sizeof(double), cudaMemcpyDeviceToHost, b->st));
-  BCU(b, cudaStreamSynchronize(b->st));
+  if ((rc = sync_and_check(b))) return rc;
   for (int k = 0; k < ns; k++) l2[b->order[k]] = b->h_l2[k];
   return AUSM_OK;
 }
 
 int ausm_batch_synchronize(ausm_batch* b) {
   BNEED(b, b, AUSM_ERR_INVALID, "null handle");
-  BCU(b, cudaStreamSynchronize(b->st));
-  return AUSM_OK;
+  return sync_and_check(b);
 }
 
 int ausm_batch_time_steps(ausm_batch* b, int n, int reps, float* ms_out) {
@@ -559,13 +584,14 @@ int ausm_batch_time_steps(ausm_batch* b, int n, int reps, float* ms_out) {
   if (rc) return rc;
   BCU(b, cudaEventRecord(b->e0, b->st));
   for (int r = 0; r < reps; r++) {
-    rc = ausm_batch_step(b, n, nullptr);
+    rc = batch_step_impl(b, n, nullptr, false);
     if (rc) return rc;
   }
   BCU(b, cudaEventRecord(b->e1, b->st));
+  if (b->tma && (rc = queue_err_read(b))) return rc;
   BCU(b, cudaEventSynchronize(b->e1));
   BCU(b, cudaEventElapsedTime(ms_out, b->e0, b->e1));
-  return AUSM_OK;
+  return sync_and_check(b);
 }
 
 }  // extern "C"

@@ -185,6 +185,8 @@ void launch_batch_residual_norm(const BatchSolve* d, int nsolves, int total_chun
   k_batch_norm<<<(nsolves + 3) / 4, 128, 0, s>>>(d, nsolves, part, l2);
 }
 
+cudaError_t set_wait_polls_batch(unsigned polls) { return cudaMemcpyToSymbol(c_wait_polls, &polls, sizeof polls); }
+
 void launch_batch_dt(BatchSolve* d, int nsolves, cudaStream_t s) {
   k_batch_dt<<<(nsolves + 127) / 128, 128, 0, s>>>(d, nsolves);
 }

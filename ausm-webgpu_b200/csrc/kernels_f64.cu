@@ -159,7 +159,7 @@ __global__ void k_ex_from_f32(const float4* __restrict__ a, V4<R>* __restrict__ 
   }
 }
 
-// surface force from the FP64 state (pressure of interior row 1, graphs.js:186-272),
+// surface force from the FP64 state (pressure of interior row 1, graphs.js:5-41),
 // per-block partial sums; Cp per wall face
 __global__ void k_ex_forces(const V4<R>* __restrict__ row1, const V2<R>* __restrict__ V, R gamma, int M,
                             double* parts, double* cp, double q_inf, double p_inf) {

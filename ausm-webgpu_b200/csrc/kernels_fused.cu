@@ -18,20 +18,15 @@
 // on the float bits, as cflReductionShaderCode ausm.js:535-581); the first step's
 // stage 1 turns it into dt.
 //
-// k_fused_tile_tma (the default) stages its tile with TMA (cp.async.bulk.tensor, no
-// multicast; tile_tma.cuh), one tile per CTA, launched with programmatic dependent
-// launch.  Two alternatives are kept for A/B timing: k_fused_stage_tma, persistent
-// CTAs with double-buffered 32 x 16 tiles (AUSM_TMA_MODE=persistent), and
-// k_fused_stage, per-thread loads of 32 x 16 tiles (AUSM_NO_TMA=1; also the residual
-// evaluation, stage 0).  Every mbarrier wait is bounded; on a timeout the CTA sets
-// *err and stops.
+// k_fused_tile_tma stages its tile with TMA (cp.async.bulk.tensor, no multicast;
+// tile_tma.cuh), one tile per CTA, launched with programmatic dependent launch.
+// k_fused_stage loads 32 x 16 tiles with per-thread loads: it evaluates the residual
+// alone (stage 0) and steps a solve whose tensor maps could not be encoded.  Every
+// mbarrier wait is bounded; on a timeout the CTA sets *err and stops.
 //
 // HBM layout: interior state float4 [N][M] (row-major, no ghost rows), face records
 // float4 Mi [N][M] and Mj [N+1][M].  Traffic per cell and stage: 16 B state in, 16 B
 // out, 16 B Qn in (stages 2 and 3), 32 B of face records.
-#include <cstdlib>
-#include <string>
-
 #include "ausm_internal.h"
 #include "stage_tile.cuh"
 #include "tile_tma.cuh"
@@ -41,17 +36,14 @@ namespace ausm {
 #ifndef AUSM_FUSED_MIN_BLOCKS
 #define AUSM_FUSED_MIN_BLOCKS 4  // resident CTAs per SM the register budget is sized for
 #endif
-#ifndef AUSM_TMA_MIN_BLOCKS
-#define AUSM_TMA_MIN_BLOCKS 3
-#endif
 
 using namespace tile;
 
-// tile height of the per-thread and persistent kernels
+// tile height of the per-thread kernel
 constexpr int TYD = 16;
 using GD = Geo<TYD>;
 
-// ---- per-thread staging, one tile per CTA (AUSM_NO_TMA=1, and the residual) ----
+// ---- per-thread staging, one tile per CTA (the residual, and solves without tensor maps) ----
 template <int SCHEME, int STAGE, bool EMIT>
 __global__ void __launch_bounds__(GD::NT, AUSM_FUSED_MIN_BLOCKS)
     k_fused_stage(const float4* __restrict__ Qs, const float4* __restrict__ Qn, float4* __restrict__ Qo,
@@ -70,141 +62,6 @@ __global__ void __launch_bounds__(GD::NT, AUSM_FUSED_MIN_BLOCKS)
   __syncthreads();
   auto qn = [&](int h) { return __ldg(&Qn[(size_t)(j0 + ty + GD::NWY * h) * M + i0 + tx]); };
   uint32_t wmax = combine_phase<STAGE, EMIT, TYD>(Ti, Tj, w, qa, qb, qn, Qo, *dtp, c, i0, j0, M, N, tx, ty);
-  if constexpr (EMIT) block_max_to(wave, wmax);
-}
-
-// ---- persistent TMA-staged version (AUSM_TMA_MODE=persistent) ----
-namespace {
-using LD = T1<TYD>;
-// dynamic shared memory layout of the persistent kernel (offsets multiples of 128 B);
-// buffers 0/1 alternate
-constexpr int BUF_BYTES = r128(LD::SQ) + r128(LD::SI) + r128(LD::SJ);
-constexpr int OFF_I = r128(LD::SQ), OFF_J = OFF_I + r128(LD::SI);  // within a buffer
-constexpr int OFF_N = 2 * BUF_BYTES;
-constexpr int OFF_BAR = OFF_N + r128(LD::SN);
-constexpr int TMA_SMEM = OFF_BAR + 128 + 128;  // + alignment slack
-}  // namespace
-
-template <int SCHEME, int STAGE, bool EMIT>
-__global__ void __launch_bounds__(GD::NT, AUSM_TMA_MIN_BLOCKS)
-    k_fused_stage_tma(const __grid_constant__ TmaMapsLaunch tm, const float4* __restrict__ Qs,
-                      float4* __restrict__ Qo, const float4* __restrict__ Mi, const float4* __restrict__ Mj,
-                      const float* __restrict__ dtp, uint32_t* __restrict__ wave, int* __restrict__ err,
-                      const Consts c, const int M, const int N, const int tilesX, const int numTiles) {
-  extern __shared__ __align__(128) unsigned char smem_raw[];
-  // TMA destinations need 16-byte (we keep 128-byte) alignment of the dynamic region
-  unsigned char* smem = smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u);
-  auto SQ = [&](int b) { return reinterpret_cast<float4(*)[GD::PW]>(smem + b * BUF_BYTES); };
-  auto SI = [&](int b) { return reinterpret_cast<float4(*)[TX + 1]>(smem + b * BUF_BYTES + OFF_I); };
-  auto SJ = [&](int b) { return reinterpret_cast<float4(*)[TX]>(smem + b * BUF_BYTES + OFF_J); };
-  float4(*SN)[TX] = reinterpret_cast<float4(*)[TX]>(smem + OFF_N);
-  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + OFF_BAR);  // [0],[1] tile buffers, [2] Qn
-
-  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * NWX + tx;
-  if (tid == 0) {
-    mbar_init(&bars[0], 1);
-    mbar_init(&bars[1], 1);
-    mbar_init(&bars[2], 1);
-    mbar_fence_init();
-  }
-  __syncthreads();
-
-  auto issue_tile = [&](int t, int buf) {  // thread 0 only
-    const int i0 = (t % tilesX) * TX, j0 = (t / tilesX) * TYD;
-    mbar_expect_tx(&bars[buf], LD::SQ + LD::SI + LD::SJ);
-    tma_load_2d(SQ(buf), &tm.qs, 4 * (i0 - 2), j0 - 2, &bars[buf]);
-    tma_load_2d(SI(buf), &tm.mi, 4 * i0, j0, &bars[buf]);
-    tma_load_2d(SJ(buf), &tm.mj, 4 * i0, j0, &bars[buf]);
-  };
-
-  const float dt = *dtp;
-  uint32_t wmax = 0u;
-  // thread 0's record of loads in flight: bit q of `pending` for barrier q, bit q of
-  // `phase` the parity of its outstanding phase
-  unsigned pending = 0u, phase = 0u;
-  bool failed = false;
-
-  if (tid == 0 && blockIdx.x < numTiles) {
-    issue_tile(blockIdx.x, 0);
-    pending |= 1u;
-  }
-  int k = 0;
-  for (int t = blockIdx.x; t < numTiles; t += gridDim.x, ++k) {
-    const int b = k & 1;
-    const int i0 = (t % tilesX) * TX, j0 = (t / tilesX) * TYD;
-    if constexpr (STAGE >= 2) {
-      if (tid == 0) {  // Qn of this tile streams in during the face phase
-        fence_proxy_async();
-        mbar_expect_tx(&bars[2], LD::SN);
-        tma_load_2d(SN, &tm.qn, 4 * i0, j0, &bars[2]);
-        pending |= 4u;
-      }
-    }
-    // ---- tile k has landed in buffer b ----
-    bool ok = mbar_wait(&bars[b], (k >> 1) & 1);
-    if (__syncthreads_or(!ok)) {
-      failed = true;
-      break;
-    }
-    if (tid == 0) {
-      pending &= ~(1u << b);
-      phase ^= 1u << b;
-    }
-    float4(*P)[GD::PW] = SQ(b);
-    float4(*Ti)[TX + 1] = SI(b);
-    float4(*Tj)[TX] = SJ(b);
-    auto stage_entry = [&](int pr, int pc) {
-      const int ig = i0 - 2 + pc, j = j0 - 2 + pr;
-      float4 q;
-      if (j >= 0 && j < N) q = (ig >= 0 && ig < M) ? P[pr][pc] : __ldg(&Qs[(size_t)j * M + wrap_i(ig, M)]);
-      else q = tile_cell(Qs, Mj, c, M, N, wrap_i(ig, M), j);
-      P[pr][pc] = to_prim<true>(q, c.gm1);
-      return q;
-    };
-    const float4 qa = stage_entry(ty + 2, tx + 2);
-    const float4 qb = stage_entry(ty + GD::NWY + 2, tx + 2);
-    for (int e = tid; e < GD::HALO; e += GD::NT) {
-      int hr, hc;
-      halo_entry<TYD>(e, hr, hc);
-      stage_entry(hr, hc);
-    }
-    if (i0 + TX >= M && tx == 0) {  // the face column past the seam (zero-filled by the box)
-      for (int r = ty; r < TYD; r += GD::NWY)
-        if (j0 + r < N) Ti[r][M - i0] = __ldg(&Mi[(size_t)(j0 + r) * M]);
-    }
-    __syncthreads();
-    // ---- prefetch the next tile into the other buffer (free since the last barrier) ----
-    if (tid == 0 && t + (int)gridDim.x < numTiles) {
-      fence_proxy_async();
-      issue_tile(t + gridDim.x, b ^ 1);
-      pending |= 1u << (b ^ 1);
-    }
-    const FaceW w = own_weights<TYD>(Ti, Tj, tx, ty);
-    faces_phase<SCHEME, TYD>(P, Ti, Tj, c, i0, j0, M, N, tx, ty);
-    __syncthreads();
-    if constexpr (STAGE >= 2) {
-      bool okn = mbar_wait(&bars[2], k & 1);
-      if (__syncthreads_or(!okn)) {
-        failed = true;
-        break;
-      }
-      if (tid == 0) {
-        pending &= ~4u;
-        phase ^= 4u;
-      }
-    }
-    auto qn = [&](int h) { return SN[ty + GD::NWY * h][tx]; };
-    wmax = max(wmax, combine_phase<STAGE, EMIT, TYD>(Ti, Tj, w, qa, qb, qn, Qo, dt, c, i0, j0, M, N, tx, ty));
-    __syncthreads();  // SN and buffer b are free for reuse
-  }
-  if (failed) {
-    if (tid == 0) {
-      atomicExch(err, 1);
-      for (int q = 0; q < 3; q++)  // let copies still in flight land before the CTA exits
-        if (pending & (1u << q)) mbar_wait(&bars[q], (phase >> q) & 1u);
-    }
-    return;
-  }
   if constexpr (EMIT) block_max_to(wave, wmax);
 }
 
@@ -240,45 +97,19 @@ void launch_tile(const float4* Qs, float4* Qo, const float4* Mi, const float4* M
              N);
 }
 
-// "AUSM_TMA_MODE=persistent" selects the persistent kernel (A/B timing)
-bool persistent_mode() {
-  static const bool persistent = [] {
-    const char* e = std::getenv("AUSM_TMA_MODE");
-    return e && std::string(e) == "persistent";
-  }();
-  return persistent;
-}
-
 template <int S, int ST, bool E>
 void launch_t(const float4* Qs, const float4* Qn, float4* Qo, const float4* Mi, const float4* Mj, float* dt,
               uint32_t* wave, int dt_mode, const Consts& c, int M, int N, const TmaMapsLaunch* tm, int ty, int* err,
               cudaStream_t s) {
-  const int tilesX = (M + TX - 1) / TX, tilesY = (N + TYD - 1) / TYD;
-  const bool persistent = persistent_mode();
   if constexpr (ST != 0) {
-    if (tm && !persistent) {
+    if (tm) {
       if (ty == 8) launch_tile<S, ST, E, 8>(Qs, Qo, Mi, Mj, dt, wave, dt_mode, c, M, N, tm, err, s);
       else if (ty == 32) launch_tile<S, ST, E, 32>(Qs, Qo, Mi, Mj, dt, wave, dt_mode, c, M, N, tm, err, s);
       else launch_tile<S, ST, E, 16>(Qs, Qo, Mi, Mj, dt, wave, dt_mode, c, M, N, tm, err, s);
       return;
     }
-    if (tm) {  // persistent, TY = 16
-      static int blocks_per_sm = 0, sms = 0;
-      auto kern = k_fused_stage_tma<S, ST, E>;
-      if (!blocks_per_sm) {
-        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, TMA_SMEM);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, kern, GD::NT, TMA_SMEM);
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        if (blocks_per_sm < 1) blocks_per_sm = 1;
-      }
-      const int numTiles = tilesX * tilesY;
-      const int grid = std::min(numTiles, blocks_per_sm * sms);
-      kern<<<grid, dim3(NWX, GD::NWY), TMA_SMEM, s>>>(*tm, Qs, Qo, Mi, Mj, dt, wave, err, c, M, N, tilesX, numTiles);
-      return;
-    }
   }
+  const int tilesX = (M + TX - 1) / TX, tilesY = (N + TYD - 1) / TYD;
   k_fused_stage<S, ST, E><<<dim3(tilesX, tilesY), dim3(NWX, GD::NWY), 0, s>>>(Qs, Qn, Qo, Mi, Mj, dt, wave, c, M, N);
 }
 template <int S>
@@ -299,7 +130,7 @@ void launch_s(int stage, bool emit, const float4* Qs, const float4* Qn, float4* 
 void launch_fused_stage(int scheme, int stage, bool emit, const float4* Qs, const float4* Qn, float4* Qo,
                         const float4* Mi, const float4* Mj, float* dt, uint32_t* wave, int dt_mode, const Consts& c,
                         int M, int N, const TmaMapsLaunch* tm, int ty, int* err, cudaStream_t s) {
-  if (dt_mode != 0 && !(tm && stage != 0 && !persistent_mode())) {  // kernels without the in-kernel time step
+  if (dt_mode != 0 && !(tm && stage != 0)) {  // kernels without the in-kernel time step
     if (dt_mode == 1) launch_dt(wave, dt, c.maxdt, c.cfl, s);
     else cudaMemsetAsync(wave, 0, sizeof(uint32_t), s);
     dt_mode = 0;
@@ -310,6 +141,9 @@ void launch_fused_stage(int scheme, int stage, bool emit, const float4* Qs, cons
     default: launch_s<2>(stage, emit, Qs, Qn, Qo, Mi, Mj, dt, wave, dt_mode, c, M, N, tm, ty, err, s); break;
   }
 }
+
+// Polls of the TMA stage kernels' first bounded waits (tma.cuh c_wait_polls).
+cudaError_t set_wait_polls_fused(unsigned polls) { return cudaMemcpyToSymbol(c_wait_polls, &polls, sizeof polls); }
 
 // Tensor maps of the TMA kernels for tile height ty: state buffers as 2-D float tensors
 // of 4M x N (row pitch 16 M bytes) with the halo box 144 x (ty+4) and the Qn box

@@ -177,7 +177,7 @@ __global__ void k_metrics_d(const double2* __restrict__ V, float4* __restrict__ 
   Mj[(size_t)j * M + i] = make_float4((float)(-ty / ld), (float)(tx / ld), (float)(0.5 * ld), w);
 }
 
-// ---- surface force (graphs.js:186-272): FP32 pressure of the first interior cell,
+// ---- surface force (graphs.js:5-41, summed as graphs.js:43-103): FP32 pressure of the first interior cell,
 // FP64 face length, normal and sum; also Cp per wall face ----
 __global__ void k_forces(const float4* __restrict__ row0, const double2* __restrict__ V, const Consts c, int M,
                          double* parts, double* cp, double q_inf, double p_inf) {

@@ -42,7 +42,7 @@ std::mutex g_scratch_mu;
 double* g_scratch_ptr[kMaxDevices] = {};
 
 // Per wall face i (vertices i, i+1 of row 0): f32 pressure of the first interior cell
-// as the reference computes it (graphs.js:196-199), FP64 length, inward normal force
+// as the reference computes it (graphs.js:26-39), FP64 length, inward normal force
 // -p l n and Cp = (p - p_inf) / q_inf.
 __global__ void k_face_forces_noalloc(const float4* __restrict__ row0, const float2* __restrict__ body, int M,
                                       float gamma, double q_inf, double p_inf, double* __restrict__ scratch) {
@@ -104,8 +104,10 @@ extern "C" int ausm_forces_noalloc(const void* wall_row, const void* body_xy, in
     return fail_na(AUSM_ERR_INVALID, "need gamma > 1, in_rho > 0, in_pressure > 0 and mach > 0");
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess || dev < 0 || dev >= kMaxDevices)
-    return fail_na(AUSM_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
+  if (e != cudaSuccess) return fail_na(AUSM_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
+  if (dev < 0 || dev >= kMaxDevices)
+    return fail_na(AUSM_ERR_INVALID, "device index " + std::to_string(dev) + " is above the " +
+                                         std::to_string(kMaxDevices) + " devices this entry point serves");
   double* scratch = nullptr;
   {
     std::lock_guard<std::mutex> lock(g_scratch_mu);

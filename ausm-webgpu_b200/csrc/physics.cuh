@@ -35,15 +35,21 @@ struct Consts {
   float h2k;       // 2 gamma/(gamma-1): twice the total enthalpy is h2k p/rho + |v|^2 (FAST only)
   float ask4;      // aStarK/4: the AUSM+-up a*^2 from twice the enthalpies (FAST only)
   float minfk;     // Vinf2/gammaInP: the AUSM+-up M_inf^2 from rho_L is rho_L * minfk (FAST only)
+  float hsg;       // sqrt(gamma)/2: the SLAU mean sound speed is hsg (sqrt(p_L/rho_L) + sqrt(p_R/rho_R)) (FAST only)
   int muscl;
 };
 
-// FAST: the hardware's approximate reciprocal and square root (PTX rcp.approx.ftz /
-// sqrt.approx.ftz, one instruction each, relative error about 1 ulp; subnormal inputs and
+// FAST: the hardware's approximate reciprocal, square root and reciprocal square root
+// (PTX rcp.approx.ftz / sqrt.approx.ftz / rsqrt.approx.ftz, one instruction each, relative error about 1 ulp; subnormal inputs and
 // results flush to zero, which no state of the solver reaches).
 __device__ __forceinline__ float rcp_approx(float b) {
   float r;
   asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(b));
+  return r;
+}
+__device__ __forceinline__ float rsqrt_approx(float b) {
+  float r;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(b));
   return r;
 }
 template <bool FAST> __device__ __forceinline__ float fdiv(float a, float b) {
@@ -64,6 +70,17 @@ template <bool FAST> __device__ __forceinline__ float fsqrt(float a) {
   }
 }
 __device__ __forceinline__ float sat(float x) { return fminf(fmaxf(x, 0.0f), 1.0f); }
+// a * b + c and a * b rounded once and clamped to [0, 1] (PTX .sat, one instruction each)
+__device__ __forceinline__ float fma_sat(float a, float b, float c) {
+  float r;
+  asm("fma.rn.sat.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+  return r;
+}
+__device__ __forceinline__ float mul_sat(float a, float b) {
+  float r;
+  asm("mul.rn.sat.f32 %0, %1, %2;" : "=f"(r) : "f"(a), "f"(b));
+  return r;
+}
 
 // Packed FP32 (sm_100 f32x2): two IEEE-rounded operations per instruction.
 __device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
@@ -289,12 +306,21 @@ __device__ __forceinline__ float4 face_flux(float4 L2, float4 L, float4 R, float
 //  - twice the total enthalpy h2 = h2k p / rho + |v|^2, so that no 0.5 |v|^2 is
 //    formed; the energy flux is h2 x (mass flux x hl);
 //  - no "+ 0" terms (those keep the reference's sign of zero in the exact path);
-//  - SLAU / SLAU2: 1/rho guarded by one max, the pressure-split functions as the cubic
-//    f(M) = (M+1)^2 (2-M) / 4 of the Mach number clamped to [-1, 1], which is exactly
-//    the reference's branch (|M| >= 1 gives 1 or 0, the cubic is 1 at M = 1, 0 at
-//    M = -1 and within [0, 1] between, so the saturate is a no-op there);
+//  - SLAU / SLAU2: 1/rho guarded by one max; one guarded p / rho per side serves both
+//    the speed of sound, a = sqrt(gamma) / 2 (sqrt(p_L / rho_L) + sqrt(p_R / rho_R)),
+//    and the enthalpy (the enthalpy takes the guarded pressure, which differs from the
+//    reference only for p < 1e-10); the pressure-split functions as the smoothstep
+//    s^2 (3 - 2 s) of s = (M + 1) / 2 clamped to [0, 1] by one saturating fused
+//    multiply-add from the normal velocity and a / 2: that is the cubic
+//    f(M) = (M+1)^2 (2-M) / 4 of the clamped Mach number, which is exactly the
+//    reference's branch (|M| >= 1 gives 1 or 0, the cubic is 1 at M = 1, 0 at M = -1
+//    and within [0, 1] between, so its saturate is a no-op); 1 - min(1, Uarc / a) and
+//    sat(-ML), sat(MR) as single saturating operations;
 //  - AUSM+-up: M_inf^2 from rho_L as rho_L Vinf^2 / (gamma p_inf); a*^2 as
 //    (aStarK / 4) (h2L + h2R), used as computed (not the square of its square root);
+//    the interface speed of sound min(a*^2 / max(uL, a*), a*^2 / max(-uR, a*)) as
+//    a*^2 / max(uL, -uR, a*) and its reciprocal as max(uL, -uR, a*) / a*^2, with a* and
+//    1 / a*^2 from one reciprocal square root (two MUFU operations instead of four);
 //    Mbar^2 = (ML^2 + MR^2) / 2 from the face Mach numbers; the K_p pressure-diffusion
 //    term only when K_p != 0 (uniform per solve; the reference's default is 0).
 template <int SCHEME>
@@ -317,11 +343,12 @@ __device__ __forceinline__ float4 face_flux_len(float4 L2, float4 L, float4 R, f
     const float h2L = fmaf(c.h2k * pL, irL, kL), h2R = fmaf(c.h2k * pR, irR, kR);
     const float Minf2 = rhoL * c.minfk;
     const float as2 = fmaxf(1e-6f, c.ask4 * (h2L + h2R));
-    const float aStar = fsqrt<true>(as2);
-    const float aHL = as2 * frcp<true>(fmaxf(uL, aStar));
-    const float aHR = as2 * frcp<true>(fmaxf(-uR, aStar));
-    const float a = fminf(aHL, aHR);
-    const float ia = frcp<true>(a);
+    // a = min(a*^2 / max(uL, a*), a*^2 / max(-uR, a*)) = a*^2 / max(uL, -uR, a*), and
+    // 1 / a = max(uL, -uR, a*) / a*^2 with 1 / a*^2 = (1 / a*)^2 from one rsqrt
+    const float rs = rsqrt_approx(as2);
+    const float mx = fmaxf(fmaxf(uL, -uR), as2 * rs);
+    const float ia = mx * (rs * rs);
+    const float a = as2 * frcp<true>(mx);
     const float ML = uL * ia, MR = uR * ia;
     const float Mbar2 = 0.5f * fmaf(MR, MR, ML * ML);
     const float Mo2 = fminf(1.0f, fmaxf(Mbar2, Minf2));
@@ -350,19 +377,19 @@ __device__ __forceinline__ float4 face_flux_len(float4 L2, float4 L, float4 R, f
     return make_float4(ml, fmaf(p1, ml, nx * Pl), fmaf(p2, ml, ny * Pl), p3 * mlh);
   } else {  // SLAU2 (SCHEME 0, Kitamura-Shima 2013) / SLAU (SCHEME 1, Shima-Kitamura 2011)
     const float irL = frcp<true>(fmaxf(rhoL, 1e-10f)), irR = frcp<true>(fmaxf(rhoR, 1e-10f));
-    const float h2L = fmaf(c.h2k * pL, irL, kL), h2R = fmaf(c.h2k * pR, irR, kR);
-    const float aL = fsqrt<true>(c.gamma * fmaxf(pL, 1e-10f) * irL);
-    const float aR = fsqrt<true>(c.gamma * fmaxf(pR, 1e-10f) * irR);
-    const float a = (aL + aR) * 0.5f;
-    const float ia = frcp<true>(a);
-    const float ML = uL * ia, MR = uR * ia;
+    // guarded p / rho: the speed of sound is sqrt(gamma p / rho), twice the enthalpy h2k p / rho + |v|^2
+    const float tL = fmaxf(pL, 1e-10f) * irL, tR = fmaxf(pR, 1e-10f) * irR;
+    const float h2L = fmaf(c.h2k, tL, kL), h2R = fmaf(c.h2k, tR, kR);
+    const float a = c.hsg * (fsqrt<true>(tL) + fsqrt<true>(tR));  // (a_L + a_R) / 2
+    const float ia = frcp<true>(a), hia = 0.5f * ia;
     const float Uarc = fsqrt<true>(0.5f * (kL + kR));
-    const float Marc = fminf(1.0f, Uarc * ia);
-    const float X = (1.0f - Marc) * (1.0f - Marc);
-    const float mL = fminf(fmaxf(ML, -1.0f), 1.0f), mR = fminf(fmaxf(-MR, -1.0f), 1.0f);
-    const float qL = fmaf(0.5f, mL, 0.5f), qR = fmaf(0.5f, mR, 0.5f);
-    const float fpp = qL * qL * (2.0f - mL);  // f(ML)
-    const float fpm = qR * qR * (2.0f - mR);  // f(-MR)
+    const float omM = fma_sat(-Uarc, ia, 1.0f);  // 1 - min(1, Uarc / a)
+    const float X = omM * omM;
+    // f(M) = (M+1)^2 (2-M) / 4 for |M| < 1, 0 or 1 beyond, is the smoothstep s^2 (3 - 2 s)
+    // of s = (M + 1) / 2 clamped to [0, 1]; f(ML) and f(-MR)
+    const float sL = fma_sat(uL, hia, 0.5f), sR = fma_sat(-uR, hia, 0.5f);
+    const float fpp = (sL * sL) * fmaf(-2.0f, sL, 3.0f);
+    const float fpm = (sR * sR) * fmaf(-2.0f, sR, 3.0f);
     const float rs = rhoL + rhoR;
     const float dpLR = pL - pR, s1 = (fpp + fpm) - 1.0f;
     float P2;  // 2 P
@@ -371,7 +398,7 @@ __device__ __forceinline__ float4 face_flux_len(float4 L2, float4 L, float4 R, f
     else
       P2 = fmaf(fpp - fpm, dpLR, fmaf(1.0f - X, s1, 1.0f) * (pL + pR));
     const float ubar = fmaf(rhoL, fabsf(uL), rhoR * fabsf(uR)) * frcp<true>(rs);
-    const float g = __saturatef(-ML) * __saturatef(MR);
+    const float g = mul_sat(-uL, ia) * mul_sat(uR, ia);  // sat(-ML) sat(MR)
     const float omg = 1.0f - g;
     const float ubo = ubar * omg;
     const float ubp = fmaf(fabsf(uL), g, ubo), ubm = fmaf(fabsf(uR), g, ubo);

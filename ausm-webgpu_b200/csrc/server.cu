@@ -11,12 +11,17 @@
 //   3. read every member's dt / wave speed and residual L2 (one synchronisation each),
 //      and retire members that converged (residual_drop decades below the initial
 //      norm), reached max_steps or diverged: forces and Cp are computed, the solver is
-//      removed and destroyed, its bytes go back to the budget.
-// All CUDA work of a server happens on the thread that pumps (the worker, or the
-// caller of ausm_server_pump / ausm_server_drain); submit and poll only touch host
-// state under the server mutex.  Rounds are counted per request from its admission,
-// so a request's dt sequence, residual checks and stopping step do not depend on what
-// else is in the batch.
+//      removed from the batch and destroyed, its bytes go back to the budget.
+// With the worker running (ausm_server_start), admission is off the rounds' path: a
+// second host thread, the admitter, prepares each admitted request (solver, grid,
+// state, first norm) on the solver's own stream while the worker keeps stepping the
+// batch on the batch stream, so their device work overlaps; the worker joins prepared
+// requests to the batch at the start of its next round (the batch stream waits for the
+// solver's stream).  A request holds its slot and budget from the moment it leaves the
+// queue.  ausm_server_pump / drain without the worker admit on the calling thread.
+// Submit and poll only touch host state under the server mutex.  Rounds are counted
+// per request from its admission, so a request's dt sequence, residual checks and
+// stopping step do not depend on what else is in the batch or when it joined.
 #include <chrono>
 #include <cmath>
 #include <condition_variable>
@@ -111,6 +116,10 @@ struct ausm_server {
   std::condition_variable cv;
   std::deque<Req*> queue;
   std::vector<Req*> active;  // in batch member order
+  std::deque<Req*> to_prepare;  // left the queue, waiting for the admitter
+  std::deque<Req*> ready;       // prepared by the admitter, joining at the next round
+  int preparing = 0;            // to_prepare + the one the admitter is working on
+  bool async_admit = false;     // the admitter thread is running
   int retiring = 0;          // finished members whose forces / teardown are in progress
   int admitting = 0;         // requests taken off the queue whose admission is in progress
   std::unordered_map<int64_t, std::unique_ptr<Req>> reqs;
@@ -118,7 +127,8 @@ struct ausm_server {
   double in_use = 0.0, peak = 0.0, cell_updates = 0.0;
   int64_t submitted = 0, rejected = 0, admitted = 0, finished = 0, failed = 0, rounds = 0;
   ausm_batch* batch = nullptr;
-  std::thread worker;
+  std::thread worker, admitter;
+  std::condition_variable admit_cv;
   bool running = false, stopping = false;
   std::string err;
 };
@@ -156,9 +166,9 @@ void finish(ausm_server* s, Req* q, int state, int stop) {
   else s->failed++;
 }
 
-// Creates the solver of q, its grid and state; on failure the request ends with the
-// library's status.
-bool admit(ausm_server* s, Req* q) {
+// Creates the solver of q, its grid and state (on the solver's own stream); on failure
+// the request ends with the library's status.
+bool prepare(ausm_server* s, Req* q) {
   const AusmRequest& r = q->r;
   ausm_solver* h = nullptr;
   int rc = ausm_create(r.M, r.N, &h);
@@ -183,19 +193,47 @@ bool admit(ausm_server* s, Req* q) {
   double l2 = NAN;
   if ((rc = ausm_residual_l2(h, &l2))) return fail_req(rc);
   q->cp.assign(r.M, NAN);
-  if (!(s->flags & AUSM_SERVE_PLAIN) && (rc = ausm_batch_add(s->batch, h))) {
+  q->l2_first = q->l2_last = l2;
+  return true;
+}
+
+// Adds a prepared request to the batch (worker thread); it is active from now on.
+bool join(ausm_server* s, Req* q) {
+  int rc;
+  if (!(s->flags & AUSM_SERVE_PLAIN) && (rc = ausm_batch_add(s->batch, q->h))) {
     q->err = ausm_batch_last_error(s->batch);
     finish(s, q, rc, 0);
     return false;
   }
   std::lock_guard<std::mutex> lk(s->mu);
-  q->l2_first = q->l2_last = l2;
   q->state = AUSM_REQ_RUNNING;
   q->t_admit = Clock::now();
   s->admitted++;
   s->admitting--;
   s->active.push_back(q);
   return true;
+}
+
+bool admit(ausm_server* s, Req* q) { return prepare(s, q) && join(s, q); }
+
+// The admitter thread: prepares requests the worker took off the queue.
+void admitter_loop(ausm_server* s) {
+  cudaSetDevice(s->dev);
+  for (;;) {
+    Req* q = nullptr;
+    {
+      std::unique_lock<std::mutex> lk(s->mu);
+      s->admit_cv.wait(lk, [&] { return s->stopping || !s->to_prepare.empty(); });
+      if (s->stopping) return;
+      q = s->to_prepare.front();
+      s->to_prepare.pop_front();
+    }
+    const bool ok = prepare(s, q);
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->preparing--;
+    if (ok) s->ready.push_back(q);
+    s->cv.notify_all();
+  }
 }
 
 // Stop decision of one member after a round.
@@ -238,23 +276,42 @@ int pump_round(ausm_server* s, int* remaining) {
     if (rc) return sfail(s, rc, ausm_batch_last_error(nullptr));
     if (s->flags & AUSM_SERVE_NO_GRAPH) ausm_batch_set_graphs(s->batch, 0);
   }
-  // 1. admission, in arrival order
+  // 1. requests the admitter has prepared join the batch; then admission, in arrival
+  // order, on this thread or handed to the admitter
   for (;;) {
     Req* q = nullptr;
     {
       std::lock_guard<std::mutex> lk(s->mu);
+      if (s->ready.empty()) break;
+      q = s->ready.front();
+      s->ready.pop_front();
+    }
+    join(s, q);
+  }
+  for (;;) {
+    Req* q = nullptr;
+    bool async;
+    {
+      std::lock_guard<std::mutex> lk(s->mu);
+      async = s->async_admit && !(s->flags & AUSM_SERVE_PLAIN);
       const int slots = (s->flags & AUSM_SERVE_PLAIN) ? 1 : s->max_active;
-      if (s->queue.empty() || (int)s->active.size() >= slots) break;
+      const int held = (int)(s->active.size() + s->ready.size()) + s->preparing;
+      if (s->queue.empty() || held >= slots) break;
       Req* f = s->queue.front();
       if (s->in_use + f->bytes > s->budget) break;
       s->queue.pop_front();
       s->in_use += f->bytes;
       f->charged = true;
-      s->admitting++;  // neither queued nor active until admit() ends
+      s->admitting++;  // neither queued nor active until it joins the batch
       if (s->in_use > s->peak) s->peak = s->in_use;
       q = f;
+      if (async) {
+        s->preparing++;
+        s->to_prepare.push_back(q);
+        s->admit_cv.notify_one();
+      }
     }
-    admit(s, q);
+    if (!async) admit(s, q);
   }
   std::vector<Req*> act;
   {
@@ -317,25 +374,33 @@ void worker_loop(ausm_server* s) {
   for (;;) {
     {
       std::unique_lock<std::mutex> lk(s->mu);
-      s->cv.wait(lk, [&] { return s->stopping || !s->queue.empty() || !s->active.empty(); });
+      // work: a batch to step, prepared requests to join, or queued requests a slot and
+      // the budget admit (otherwise wait for a retirement, a preparation or a submit)
+      auto work = [&] {
+        if (s->stopping || !s->active.empty() || !s->ready.empty()) return true;
+        if (s->queue.empty()) return false;
+        const int slots = (s->flags & AUSM_SERVE_PLAIN) ? 1 : s->max_active;
+        return (int)s->ready.size() + s->preparing < slots && s->in_use + s->queue.front()->bytes <= s->budget;
+      };
+      s->cv.wait(lk, work);
       if (s->stopping) return;
     }
     int left = 0;
-    if (pump_round(s, &left) != AUSM_OK) {
-      // a device error ends every request still on the server
-      std::vector<Req*> all;
+    const int rc = pump_round(s, &left);
+    if (rc != AUSM_OK) {
+      // a round failed: its batch members end with the round's status; queued requests
+      // stay queued (a broken device fails them at their own admission)
+      std::vector<Req*> act;
       std::string why;
       {
         std::lock_guard<std::mutex> lk(s->mu);
-        all.assign(s->active.begin(), s->active.end());
-        all.insert(all.end(), s->queue.begin(), s->queue.end());
+        act.assign(s->active.begin(), s->active.end());
         s->active.clear();
-        s->queue.clear();
         why = s->err;
       }
-      for (Req* q : all) {
+      for (Req* q : act) {
         q->err = why;
-        finish(s, q, AUSM_ERR_CUDA, 0);
+        finish(s, q, rc, 0);
       }
       std::lock_guard<std::mutex> lk(s->mu);
       s->cv.notify_all();
@@ -375,11 +440,24 @@ int ausm_server_stop(ausm_server* s) {
     if (!s->running) return AUSM_OK;
     s->stopping = true;
     s->cv.notify_all();
+    s->admit_cv.notify_all();
   }
   s->worker.join();
+  if (s->admitter.joinable()) s->admitter.join();
   std::lock_guard<std::mutex> lk(s->mu);
   s->running = false;
   s->stopping = false;
+  s->async_admit = false;
+  // requests handed to the admitter but not prepared go back to the front of the queue
+  while (!s->to_prepare.empty()) {
+    Req* q = s->to_prepare.back();
+    s->to_prepare.pop_back();
+    s->preparing--;
+    s->admitting--;
+    s->in_use -= q->bytes;
+    q->charged = false;
+    s->queue.push_front(q);
+  }
   return AUSM_OK;
 }
 
@@ -387,7 +465,9 @@ int ausm_server_destroy(ausm_server* s) {
   if (!s) return AUSM_OK;
   ausm_server_stop(s);
   if (s->dev >= 0) cudaSetDevice(s->dev);
-  for (Req* q : s->active)
+  std::vector<Req*> held(s->active.begin(), s->active.end());
+  held.insert(held.end(), s->ready.begin(), s->ready.end());
+  for (Req* q : held)
     if (q->h) {
       if (q->h->batch) ausm_batch_remove(q->h->batch, q->h);
       ausm_destroy(q->h);
@@ -453,10 +533,12 @@ int ausm_server_start(ausm_server* s) {
     return sfail(nullptr, AUSM_ERR_CUDA, "no CUDA device");
   }
   s->running = true;
+  s->async_admit = !(s->flags & AUSM_SERVE_PLAIN);
   s->worker = std::thread([s] {
     cudaSetDevice(s->dev);
     worker_loop(s);
   });
+  if (s->async_admit) s->admitter = std::thread([s] { admitter_loop(s); });
   return AUSM_OK;
 }
 

@@ -39,6 +39,7 @@ struct ausm_solver {
   double* parts = nullptr;  // 2 * kMaxParts per-block partial sums
   uint32_t* move = nullptr;
   int* err_flag = nullptr;  // set by a kernel whose bounded wait gave up
+  bool err_read_queued = false;  // a copy of *err_flag to h_wave[2] is queued on st (api.cu)
   ausm::TmaMaps tma[3];  // per tile height kTileHeights[k]
   int tile_rows = 0;      // tile height of the TMA stage kernel; 0 until tuned
   float* h_dt = nullptr;

@@ -76,7 +76,7 @@ template <int STAGE, int TY>
 __device__ __forceinline__ bool tile_tma_wait(unsigned char* smem, int q, int tid, int* err) {
   uint64_t* bar = reinterpret_cast<uint64_t*>(smem + T1<TY>::OFF_BAR);
   bool ok = true;
-  if (tid == 0) ok = mbar_wait(&bar[q], 0);
+  if (tid == 0) ok = mbar_wait(&bar[q], 0, c_wait_polls);
   if (__syncthreads_or(!ok)) {
     if (tid == 0) {
       atomicExch(err, 1);

@@ -47,11 +47,19 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
       : "memory");
   return ok != 0;
 }
-// Bounded wait for the phase with the given parity; false when it gave up.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity) {
-  for (unsigned it = 0; it < kWaitPolls; ++it)
+// Bounded wait for the phase with the given parity: at most `polls` polls (none for
+// polls = 0); false when it gave up.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity, unsigned polls = kWaitPolls) {
+  for (unsigned it = 0; it < polls; ++it)
     if (mbar_try_wait(bar, parity)) return true;
   return false;
 }
+
+// Polls of a tile's first wait for each of its boxes (kWaitPolls).  Tests lower it
+// (ausm_debug_set_wait_polls, to 0: the wait gives up at once) to drive the timeout
+// path without a fault: the tile then reports AUSM_ERR_TIMEOUT and still waits, with
+// the full bound, for its copies to land before the CTA exits.  One copy per
+// translation unit that launches TMA stage kernels, each with its own setter.
+static __constant__ unsigned c_wait_polls = kWaitPolls;
 
 }  // namespace ausm

@@ -41,6 +41,7 @@ sys.path.insert(0, str(ROOT / "ausm-webgpu_b200"))
 WORKLOAD = dict(name="naca0024_4096x3072_m6_aoa4_slau2", naca=24, M=4096, N=3072, far_chords=40.0,
                 first_spacing=1e-3, mach=6.0, aoa_deg=4.0, scheme="SLAU2", cfl=0.5, grid_iters=200)
 ALG_BYTES_PER_CELL_STEP = 152  # 3 stages x (16 in + 16 out) + 2 x 16 Qn + 3 x 8 vertex
+TIMED_S = 1.5  # seconds of repeated timed regions (the median region is reported)
 METRIC = "Mcell-updates/s per RK3 step"
 
 # 64 independent O-grids, cells log-uniform from 128x96 to 1024x768 (aspect 4:3), random
@@ -91,8 +92,9 @@ class Clocks:
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
          "clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, gpu_index: int):
+    def __init__(self, gpu_index: int, interval_ms: int = 50):
         self.idx = gpu_index
+        self.ms = interval_ms
         self.proc = None
         self.f = None
 
@@ -100,7 +102,7 @@ class Clocks:
         try:
             self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
             self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
-                                          "-i", str(self.idx), "-lms", "200"], stdout=self.f,
+                                          "-i", str(self.idx), "-lms", str(self.ms)], stdout=self.f,
                                          stderr=subprocess.DEVNULL)
         except (OSError, FileNotFoundError):
             self.proc = None
@@ -352,8 +354,32 @@ def run_batched(ausm, cfg, warmup, plain=True):
             "sizes": f"{min(sp['M'] * sp['N'] for sp in specs)}..{max(sp['M'] * sp['N'] for sp in specs)} cells"}
 
 
+def workload_grid_host(wl, M=None, N=None):
+    """The workload's O-grid built on the host cores with the library's generator restated
+    in the oracle (test infrastructure): NACA body (chord 1 at the origin), circular far
+    field, the geometric radial stretch (oracle/geometry_ref.stretched_guess) and
+    wl['grid_iters'] multicolour TTM sweeps in double (the oracle's restatement of the
+    library's FP64 generator), rounded to float32.  Used by the CPU legs only."""
+    import numpy as np
+    from oracle.geometry_ref import circular_outer, naca4_boundary, stretched_guess
+    from oracle.oracle import Oracle
+    M = M or wl["M"]
+    N = N or wl["N"]
+    body = naca4_boundary(M, wl["naca"], 0.5, 0.0)
+    outer = circular_outer(M, wl["far_chords"])
+    o = Oracle(M, N, "f64")
+    o.set_vertices(stretched_guess(body, outer, N, wl["first_spacing"]))
+    o.grid_multicolor(wl["grid_iters"], 0.0)
+    v = o.vertices().astype(np.float32)
+    o.close()
+    return v
+
+
 def cpu_reference_sample(wl, vertices=None, target_s=20.0, K=1):
-    """Time the reference's step on the host cores (oracle/_ref, else the oracle port)."""
+    """Time the reference's step on the host cores (oracle/_ref, else the oracle port).
+    The sample is the whole workload grid when K steps of it fit in target_s seconds at
+    the probed host rate (vertices: the GPU run's grid; None: built on the host with the
+    same generator), else a sub-grid of the same flow on a linear-interpolation grid."""
     import numpy as np
     from oracle.oracle import Oracle, RefWGSL, make_params, oracle_lib, ref_available
     from oracle.geometry_ref import naca4_boundary, circular_outer
@@ -385,20 +411,23 @@ def cpu_reference_sample(wl, vertices=None, target_s=20.0, K=1):
 
     # probe the host rate on a small grid, then size the sample
     obj, fn = make(256, 192, None)
+    fn(1)
     t = time.perf_counter()
     fn(1)
     rate = 256 * 192 / (time.perf_counter() - t)
     del obj
     cells_budget = rate * target_s / max(K, 1)
-    if vertices is not None and wl["M"] * wl["N"] <= cells_budget:
-        M, N, verts = wl["M"], wl["N"], vertices
+    same = wl["M"] * wl["N"] <= cells_budget
+    if same:
+        M, N = wl["M"], wl["N"]
+        verts = vertices if vertices is not None else workload_grid_host(wl)
     else:
         scale = max(min(math.sqrt(cells_budget / (wl["M"] * wl["N"])), 1.0), 1 / 32)
         M = max(32, int(wl["M"] * scale) // 4 * 4)
         N = max(24, int(wl["N"] * scale) // 3 * 3)
         verts = None
     obj, fn = make(M, N, verts)
-    return kind, M, N, fn, obj
+    return kind, M, N, fn, obj, same
 
 
 def threads_used():
@@ -414,8 +443,8 @@ def run_reference_arm(args):
     if rank != 0:
         return 0
     wl = WORKLOAD
-    target = max(10.0, min(150.0, 0.15 * args.steps))
-    kind, M, N, fn, obj = cpu_reference_sample(wl, None, target_s=target, K=args.steps + args.warmup)
+    # the whole run (warm-up and timed steps) within about two and a half minutes
+    kind, M, N, fn, obj, same = cpu_reference_sample(wl, None, target_s=150.0, K=args.steps + args.warmup)
     for _ in range(args.warmup):
         fn(1)
     t = time.perf_counter()
@@ -428,7 +457,9 @@ def run_reference_arm(args):
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "Mcell-updates/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": el / args.steps * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": wl["name"], "sample_grid": f"{M}x{N}", "parallelism": "host cores"},
+            "config": {"workload": wl["name"], "sample_grid": f"{M}x{N}", "same_config": same,
+                       "grid": "the workload's stretched O-grid, 200 multicolour sweeps, built on the host" if same
+                       else "linear-interpolation sub-grid", "parallelism": "host cores"},
             "cpu_baseline": {"value": value, "unit": "Mcell-updates/s", "cores": threads_used(), "kind": kind,
                              "sample": sample},
             "e2e": {"value": value, "unit": "Mcell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -498,19 +529,28 @@ def main():
     M, N = s.M, s.N
     cells = M * N
 
-    for _ in range(args.warmup):
-        s.step(1, wait=False)
-    s.synchronize()
-    if dist:
-        dist.barrier()
+    # The clock sampler runs from before the warm-up to the end of the timed regions.  The
+    # timed region (K steps, CUDA events on the solver's stream, synchronised, barrier
+    # first) is repeated until about TIMED_S seconds have passed, so that the clock record
+    # covers it; the median region counts.  Every rank repeats it the same number of times.
     with Clocks(local_rank) as clk:
-        t0 = time.perf_counter()
-        ms = s.time_steps(1, args.steps)  # CUDA events on the solver's stream, synchronised
-        wall = time.perf_counter() - t0
+        for _ in range(args.warmup):
+            s.step(1, wait=False)
+        s.synchronize()
+        probe = s.time_steps(1, args.steps)
+        reps = int(max_over_ranks(max(3, min(500, math.ceil(TIMED_S * 1e3 / max(probe, 1e-3)))), dist))
+        times, walls = [], []
+        for _ in range(reps):
+            if dist:
+                dist.barrier()
+            t0 = time.perf_counter()
+            times.append(s.time_steps(1, args.steps))
+            walls.append(time.perf_counter() - t0)
     clocks = clk.summary()
     dt_check = s.step(0)  # raises if the run diverged
-    times = [ms]
-    ms = max_over_ranks(ms, dist)
+    ms_med = statistics.median(times)
+    ms = max_over_ranks(ms_med, dist)
+    wall = statistics.median(walls)
     value = world * cells * args.steps / (ms * 1e-3) / 1e6
 
     # end to end through the public API with pinned host buffers
@@ -538,7 +578,7 @@ def main():
                        f"from/to pinned host memory", "calls": args.e2e_calls}
 
     peak, peak_kind = peaks()
-    achieved = cells * ALG_BYTES_PER_CELL_STEP * args.steps / (times[0] * 1e-3) / 1e9
+    achieved = cells * ALG_BYTES_PER_CELL_STEP * args.steps / (ms_med * 1e-3) / 1e9
     traffic = traffic_from_profile(cells)
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": traffic, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind ==
@@ -550,7 +590,7 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             verts = s.vertices()
-            kind, cM, cN, fn, obj = cpu_reference_sample(wl, verts, target_s=args.cpu_seconds, K=2)
+            kind, cM, cN, fn, obj, _ = cpu_reference_sample(wl, verts, target_s=args.cpu_seconds, K=2)
             fn(1)
             t0 = time.perf_counter()
             fn(2)
@@ -563,7 +603,7 @@ def main():
             L, n0 = oracle_lib(), threads_used()
             L.orc_set_num_threads(1)
             try:
-                kind1, M1, N1, fn1, obj1 = cpu_reference_sample(wl, None, target_s=max(2.0, args.cpu_seconds / 3), K=1)
+                kind1, M1, N1, fn1, obj1, _ = cpu_reference_sample(wl, None, target_s=max(2.0, args.cpu_seconds / 3), K=1)
                 t0 = time.perf_counter()
                 fn1(1)
                 el1 = time.perf_counter() - t0
@@ -588,7 +628,8 @@ def main():
                 "config": {"workload": wl["name"], "cells": cells, "grid": f"{M}x{N}", "engine": args.engine,
                            "parallelism": f"replicas{world}", "l2": ("inputs larger than L2" if cells * 16 > 126e6 else "inputs fit in L2") +
                            f" ({cells * 16 / 1e6:.0f} MB state, {cells * 32 / 1e6:.0f} MB face records)",
-                           "wall_s": wall},
+                           "wall_s": wall, "timed_regions": len(times),
+                           "ms_per_step_min_max": [min(times) / args.steps, max(times) / args.steps]},
                 # per step(1): fused, three stage kernels (dt is computed in stage 1); reference,
                 # 5 dispatches per stage, the dt kernel and the wave-speed reduction
                 "gpu_launches": (3 if args.engine == "fused" else 17) * args.steps, "clocks": clocks, "roofline": roofline, "cpu_baseline": cpu,

@@ -153,11 +153,15 @@ int ausm_get_state_f64(ausm_solver* h, double* q);
 
 /* step(n): dt = min(maxdt, cfl / max wave speed) of the current state, held for n
  * TVD-RK3 steps, then the max wave speed of the new state (main.js:744-791).  dt_out
- * may be NULL (then the call does not wait for the GPU). */
+ * may be NULL (then the call does not wait for the GPU).  A tile whose bounded wait
+ * gave up (AUSM_ERR_TIMEOUT) is reported by this call when it waits (dt_out given),
+ * else by the next call on the handle that waits for the GPU (get_state, forces,
+ * residual_l2, field, max_wave_speed, synchronize, time_steps or a step with dt_out). */
 int ausm_step(ausm_solver* h, int n, float* dt_out);
 int ausm_max_wave_speed(ausm_solver* h, float* out);
 
-/* Surface force (graphs.js:186-272) with FP64 accumulation: out[6] = Fx, Fy,
+/* Surface force (per wall face graphs.js:5-41, sum and coefficients graphs.js:43-103)
+ * with FP64 accumulation: out[6] = Fx, Fy,
  * |F| sign(F.V), Cl, Cd, Cl/Cd (coefficients per the reference, not divided by chord);
  * cp (may be NULL) gets M wall pressure coefficients (p - p_inf) / q_inf. */
 int ausm_forces(ausm_solver* h, double* out6, double* cp);
@@ -188,6 +192,13 @@ int ausm_synchronize(ausm_solver* h);
 /* Device-timed loop for benchmarks: `reps` calls of step(n) bracketed by CUDA events
  * on the handle's stream; ms_out gets the elapsed device time of all of them. */
 int ausm_time_steps(ausm_solver* h, int n, int reps, float* ms_out);
+/* Test hook (no counterpart in the reference): the number of polls, 0 to 65536 (the
+ * default), of the first bounded wait of every TMA box of the stage kernels on the
+ * current device, in this process.  0 makes every such wait give up at once, so a test
+ * can drive the timeout path without a fault: the tiles report AUSM_ERR_TIMEOUT, write
+ * nothing, and still let their copies land (second wait, full bound) before they exit.
+ * Restore 65536 afterwards. */
+int ausm_debug_set_wait_polls(unsigned polls);
 /* Tile-height autotuner of the fused engine (no counterpart in the reference): times
  * the TMA stage kernel for tiles of 32 x 8, 32 x 16 and 32 x 32 cells on this solve's
  * grid and state and keeps the fastest for its steps (cached per M, N and scheme for the

@@ -396,7 +396,7 @@ template <class T> struct Oracle {
     return d;
   }
 
-  // surface force (graphs.js:186-210) and its 256-lane tree sum (graphs.js:232-272)
+  // surface force (graphs.js:5-41) and its 256-lane tree sum (graphs.js:43-103)
   void forces(double* out /* Fx, Fy, |F|sign(F.V), Cl, Cd, Cl/Cd */) {
     std::vector<V2<T>> f(M);
     for (int i = 0; i < M; i++) {
@@ -492,6 +492,9 @@ template <class T> struct Oracle {
       mv = T(0);
       int ncol = odd ? 6 : 4;
       for (int c = 0; c < ncol; c++) {
+        // the points of one colour do not touch each other: any order gives the same result
+        T cmv = T(0);
+#pragma omp parallel for schedule(static) reduction(max : cmv)
         for (int j = 1; j < N; j++)
           for (int i = 0; i < M; i++) {
             int col;
@@ -501,9 +504,10 @@ template <class T> struct Oracle {
             V2<T> p = ttm_point(vtx, i, j);
             size_t k = ((size_t)j * M + i) * 2;
             T d = wmax(std::fabs(p.x - vtx[k]), std::fabs(p.y - vtx[k + 1]));
-            mv = wmax(mv, d);
+            cmv = wmax(cmv, d);
             vtx[k] = p.x; vtx[k + 1] = p.y;
           }
+        mv = wmax(mv, cmv);
       }
       sweeps++;
       if (mv <= tol) break;

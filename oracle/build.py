@@ -20,6 +20,8 @@ from pathlib import Path
 HERE = Path(__file__).resolve().parent
 BUILD = HERE / "_build"
 REF_OUT = HERE / "_ref"
+# The reference tree: AUSM_REFERENCE_ROOT, else where this build recipe finds it in the
+# build container.  This recipe is the one place that names that location.
 REF_SRC = Path(os.environ.get("AUSM_REFERENCE_ROOT", "/root/reference"))
 
 CXXFLAGS = ["-O2", "-ffp-contract=off", "-fno-fast-math", "-fopenmp", "-fPIC", "-Wall", "-Wno-unused"]

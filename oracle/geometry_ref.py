@@ -75,3 +75,40 @@ def rectangular_outer(M: int, length_ratio: float = 1.5) -> np.ndarray:
 def circular_outer(M: int, radius: float = 1.0) -> np.ndarray:
     t = np.arange(M, dtype=np.float64) / M
     return np.stack([radius * np.cos(t * np.pi * 2), radius * np.sin(t * np.pi * 2)], axis=1)
+
+
+def stretched_guess(body, outer, N: int, first_spacing: float) -> np.ndarray:
+    """(N+1, M, 2) float64 initial guess of an O-grid between the body (row 0) and the far
+    field (row N): along each column t(j) = h (q^j - 1) / (q - 1) with h = first_spacing / L
+    (L the column's length) and q found by bisection so that t(N) = 1; first_spacing <= 0
+    gives t = j / N (the reference's linear interpolation, shaders/grid.js:24-27).  This
+    restates the library's geometric radial stretching (k_grid_init_d) in double."""
+    body = np.asarray(body, np.float64)
+    outer = np.asarray(outer, np.float64)
+    M = body.shape[0]
+    V = np.zeros((N + 1, M, 2))
+    V[0], V[N] = body, outer
+    j = np.arange(1, N, dtype=np.float64)
+    for i in range(M):
+        a, b = body[i], outer[i]
+        if first_spacing <= 0.0:
+            t = j / N
+        else:
+            L = math.sqrt((b[0] - a[0]) ** 2 + (b[1] - a[1]) ** 2)
+            h = first_spacing / L
+            lo, hi = 1.0 + 1e-12, 2.0
+            if h * N >= 1.0:
+                lo, hi = 1e-6, 1.0 - 1e-12
+            for _ in range(200):
+                q = 0.5 * (lo + hi)
+                sN = h * (math.pow(q, N) - 1.0) / (q - 1.0)
+                if (sN > 1.0) == (h * N < 1.0):
+                    hi = q
+                else:
+                    lo = q
+            q = 0.5 * (lo + hi)
+            qj = np.array([math.pow(q, k) for k in range(1, N)])  # libm pow, as the scalar form
+            t = h * (qj - 1.0) / (q - 1.0)
+        V[1:N, i, 0] = a[0] * (1.0 - t) + b[0] * t
+        V[1:N, i, 1] = a[1] * (1.0 - t) + b[1] * t
+    return V

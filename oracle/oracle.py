@@ -112,6 +112,7 @@ def ref_lib():
             ("set_state", [C.c_void_p, F], None), ("frame", [C.c_void_p, C.c_int], C.c_double),
             ("eval_residual", [C.c_void_p], None), ("forces", [C.c_void_p, C.POINTER(C.c_double)], None),
             ("max_wave_bits", [C.c_void_p], C.c_uint32), ("get_wave_speeds", [C.c_void_p, F], None),
+            ("field", [C.c_void_p, C.c_int, F], None),
             ("texture_size", [C.c_void_p, C.c_int], C.c_longlong), ("get_texture", [C.c_void_p, C.c_int, F], None),
         ]:
             f = getattr(L, f"ref_{name}")
@@ -218,7 +219,7 @@ class Oracle:
         return fx, fy
 
     def forces(self):
-        """Fx, Fy, |F| sign(F.V), Cl, Cd, Cl/Cd (graphs.js:257-270)."""
+        """Fx, Fy, |F| sign(F.V), Cl, Cd, Cl/Cd (graphs.js:87-100)."""
         out = (C.c_double * 6)()
         self._f("forces")(self.h, out)
         return np.array(list(out))
@@ -301,6 +302,16 @@ class RefWGSL:
     def wave_speeds(self):
         a = np.zeros((self.N, self.M), dtype=np.float32)
         self.L.ref_get_wave_speeds(self.h, _ptr(a, C.c_float))
+        return a
+
+    # display modes of the visualization shader (ausm.js:667-695) with a raw field value
+    FIELD_MODES = {"density": 2, "temperature": 3, "pressure": 4, "mach": 5, "entropy": 8}
+
+    def field(self, name: str):
+        """The visualization shader's raw value of a field for state2 (M x N, before the
+        colour map), from translate.py's field probe of the reference's shader."""
+        a = np.zeros((self.N, self.M), dtype=np.float32)
+        self.L.ref_field(self.h, self.FIELD_MODES[name], _ptr(a, C.c_float))
         return a
 
     TEX = {"gridPoints0": (0, 2), "gridPoints1": (1, 2), "gridArea": (2, 1), "faceLengths": (3, 4),

@@ -32,6 +32,7 @@ DECL_MOD(integrationStage2ShaderCode)
 DECL_MOD(integrationStage3ShaderCode)
 DECL_MOD(cflReductionShaderCode)
 DECL_MOD(visualizationShaderCode)
+DECL_MOD(visualizationFieldProbe)
 DECL_MOD(gridInterpolationShaderCode)
 DECL_MOD(gridEllipticPoissonShaderCode)
 DECL_MOD(gridFinalizeShaderCode)
@@ -187,6 +188,19 @@ struct RefSim {
     c.bind(0, &uni); c.bind(1, waveSpeeds.data()); c.bind(2, &maxWaveSpeed);
     c.dispatch((unsigned)(((long long)M * N + 255) / 256), 1, 1);
   }
+  // Raw field value of display mode `mode` (2 density, 3 temperature, 4 pressure,
+  // 5 Mach, 8 entropy) of state2 from the visualization shader's own arithmetic
+  // (translate.py's field probe), M x N floats.
+  void field(int mode, float* out) {
+    std::vector<float> buf((size_t)M * N, 0.0f);
+    Uniforms u = uni;
+    u.simDisplayMode = (float)mode;
+    Mod v = MOD(visualizationFieldProbe);
+    v.bind(0, &u); v.bind(1, &state2); v.bind(2, &faceLengths); v.bind(3, &gridArea);
+    v.bind(4, &vis); v.bind(5, buf.data());
+    v.dispatch(wg(M), wg(N), 1);
+    std::memcpy(out, buf.data(), buf.size() * sizeof(float));
+  }
   // prepareState (main.js:631-655); mode 1 starts from uni.inState everywhere instead of
   // the reference's fluid at rest (new option for freestream starts).
   void prepare_state(int mode) {
@@ -259,7 +273,7 @@ struct RefSim {
     fluxes(state0);
     residual_pass();
   }
-  // force calc + integration (main.js:808-810, graphs.js:186-272)
+  // force calc + integration (main.js:808-810, graphs.js:5-103)
   void forces(double* out) {
     Mod f = MOD(forceCalcShaderCode);
     f.bind(0, &uni); f.bind(1, &state2); f.bind(2, &gridPoints0); f.bind(3, forceValues.data());
@@ -295,6 +309,7 @@ double ref_frame(void* h, int steps) { return static_cast<RefSim*>(h)->frame(ste
 void ref_eval_residual(void* h) { static_cast<RefSim*>(h)->eval_residual(); }
 void ref_forces(void* h, double* out) { static_cast<RefSim*>(h)->forces(out); }
 uint32_t ref_max_wave_bits(void* h) { return static_cast<RefSim*>(h)->maxWaveSpeed; }
+void ref_field(void* h, int mode, float* out) { static_cast<RefSim*>(h)->field(mode, out); }
 void ref_get_wave_speeds(void* h, float* w) {
   auto* r = static_cast<RefSim*>(h);
   std::memcpy(w, r->waveSpeeds.data(), r->waveSpeeds.size() * sizeof(float));

@@ -608,6 +608,24 @@ MODULES = {
 }
 
 
+# Field probe: the reference's visualization shader with its final colour-mapped store
+# replaced by a store of the raw field value of the display mode (density, temperature,
+# pressure, Mach, entropy) into the shader's own f32 buffer (binding 5), so that the
+# headless field outputs can be compared with the reference's own arithmetic.  One
+# statement is rewritten; everything before it is the reference's text.
+PROBE_SRC = "visualizationShaderCode"
+PROBE_NAME = "visualizationFieldProbe"
+PROBE_FROM = ("textureStore(vis, gid.xy, colorMapBRYW(((localValue - freeStreamValue) * uni.visMultiplier)"
+              " / (freeStreamValue * 2) + 0.5));")
+PROBE_TO = "waveSpeeds[gid.x + gid.y * u32(uni.simDomain.x)] = localValue;"
+
+
+def probe_source(wgsl: str) -> str:
+    if wgsl.count(PROBE_FROM) != 1:
+        raise ValueError("field probe: the visualization shader's final store was not found exactly once")
+    return wgsl.replace(PROBE_FROM, PROBE_TO)
+
+
 def uniforms_header(uni_fields, guni_fields):
     out = ["#pragma once", '#include "wgsl_rt.h"', "namespace wgsl {"]
     for sname, fields in (("Uniforms", uni_fields), ("GraphUniforms", guni_fields)):
@@ -640,11 +658,17 @@ def translate_reference(ref_root: Path, out_dir: Path):
             p = out_dir / f"{name}.cpp"
             p.write_text(cpp)
             written.append(p)
+    wgsl = probe_source(tpl.expand(PROBE_SRC))
+    p = out_dir / f"{PROBE_NAME}.cpp"
+    p.write_text(Module(PROBE_NAME, wgsl, overrides, uni_fields, guni_fields).translate())
+    written.append(p)
     return written
 
 
 if __name__ == "__main__":
-    ref = Path(sys.argv[1]) if len(sys.argv) > 1 else Path("/root/reference")
+    if len(sys.argv) < 2:
+        sys.exit("usage: translate.py REFERENCE_ROOT [OUT_DIR]")
+    ref = Path(sys.argv[1])
     out = Path(sys.argv[2]) if len(sys.argv) > 2 else Path(__file__).resolve().parents[1] / "_ref" / "gen"
     for p in translate_reference(ref, out):
         print(p)

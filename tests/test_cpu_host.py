@@ -13,7 +13,7 @@ import pytest
 from ausm import _lib, geometry
 from oracle.geometry_ref import circular_outer, naca4_boundary, rectangular_outer
 
-REF = Path(os.environ.get("AUSM_REFERENCE_ROOT", "/root/reference"))
+from oracle.build import REF_SRC as REF  # the reference tree, where the oracle's build recipe finds it
 
 
 def test_library_exports_every_header_function():

@@ -1,0 +1,152 @@
+"""Parity on the benchmark configurations themselves, against the oracle and the
+reference's own shaders, through the C ABI (tests/baseline_cases.py has the inputs).
+
+Configuration 1 (NACA 0012, 256 x 128, M 0.5, SLAU2):
+  - one step: the fused engine against the float32 oracle, normwise <= 1e-5 (as the
+    golden-case gate); the reference-shaped engine bit for bit;
+  - the configuration's 2000 steps (frames of 100): against the reference's own shaders
+    (tests/golden/baseline_c1.npz), density relative L2 and wall Cp (max difference over
+    max |Cp|) <= 1e-4 for the fused engine, bit for bit for the reference-shaped engine;
+  - the converged run (frames of 500 after that, to a 4-decade density-residual drop or
+    the served configuration's 50000-step limit, whichever comes first; the fixture
+    records where the reference stopped): density L2 and wall Cp within the bound below.
+Configuration 2 (NACA 2412, 512 x 384; M 0.8 SLAU2, M 2 AUSM+-up, M 8 SLAU): one step
+  at 1e-5 and 300 steps (frames of 100) at 1e-4 normwise against the float32 oracle run
+  on the host cores in the test.
+"""
+import hashlib
+import math
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from baseline_cases import CONFIG1, CONFIG2, density_l2_rel, flow_kwargs, make_grid, wall_cp
+from test_gpu_parity import normwise
+
+pytestmark = pytest.mark.gpu
+
+TOL_STEP1 = 1e-5
+TOL_RUN = 1e-4
+GOLDEN = Path(__file__).resolve().parent / "golden" / "baseline_c1.npz"
+
+_grids = {}
+
+
+def grid(cfg):
+    key = (cfg["M"], cfg["N"], cfg["naca"])
+    if key not in _grids:
+        _grids[key] = make_grid(cfg)
+    return _grids[key]
+
+
+@pytest.fixture(scope="module")
+def c1():
+    g = dict(np.load(GOLDEN))
+    v = grid(CONFIG1)
+    assert hashlib.sha256(v.tobytes()).hexdigest() == str(g["grid_sha256"][0]), "grid differs from the fixture's"
+    return g, v
+
+
+def solver(cfg, v, run, engine="fused"):
+    from ausm import Solver
+    s = Solver(cfg["M"], cfg["N"], engine=engine)
+    s.set_vertices(v)
+    s.set_params(**flow_kwargs(run, cfg["cfl"]))
+    s.prepare_state("freestream")
+    return s
+
+
+def oracle(cfg, v, run):
+    from oracle.oracle import Oracle, make_params
+    o = Oracle(cfg["M"], cfg["N"], "f32")
+    o.set_params(make_params(mach=run["mach"], aoa_deg=run["aoa_deg"], scheme=run["scheme"], cfl=cfg["cfl"]))
+    o.set_vertices(v)
+    o.metrics()
+    o.init_state(1)
+    return o
+
+
+def advance(s, steps, frame):
+    done = 0
+    while done < steps:
+        n = min(frame, steps - done)
+        s.step(n)
+        done += n
+
+
+def test_config1_one_step(c1):
+    _, v = c1
+    N = CONFIG1["N"]
+    o = oracle(CONFIG1, v, CONFIG1)
+    dt_ref = o.step(1)
+    ref = o.state()[1:N + 1]
+    o.close()
+    for engine in ("fused", "reference"):
+        s = solver(CONFIG1, v, CONFIG1, engine)
+        dt = s.step(1)
+        q = s.state()[1:N + 1]
+        s.close()
+        if engine == "reference":
+            assert np.array_equal(q, ref) and np.float32(dt) == np.float32(dt_ref)
+        else:
+            err = normwise(q, ref)
+            assert err <= TOL_STEP1, f"normwise {err:.3e}"
+            assert abs(dt - dt_ref) <= 1e-5 * dt_ref
+
+
+@pytest.mark.parametrize("engine", ["fused", "reference"])
+def test_config1_2000_steps(c1, engine):
+    g, v = c1
+    N = CONFIG1["N"]
+    s = solver(CONFIG1, v, CONFIG1, engine)
+    advance(s, CONFIG1["steps"], CONFIG1["frame"])
+    q = s.state()
+    f = s.forces(with_cp=True)
+    s.close()
+    rho = q[1:N + 1, :, 0]
+    if engine == "reference":
+        assert np.array_equal(rho, g["rho_2000"])
+        assert np.array_equal(wall_cp(q[1], CONFIG1["mach"]), g["cp_2000"])
+        return
+    d_rho = density_l2_rel(rho, g["rho_2000"])
+    d_cp = np.abs(f["Cp"] - g["cp_2000"]).max() / np.abs(g["cp_2000"]).max()
+    assert d_rho <= TOL_RUN, f"density relative L2 {d_rho:.3e}"
+    assert d_cp <= TOL_RUN, f"wall Cp {d_cp:.3e} of max |Cp|"
+
+
+def test_config1_converged(c1):
+    g, v = c1
+    N = CONFIG1["N"]
+    s = solver(CONFIG1, v, CONFIG1)
+    advance(s, CONFIG1["steps"], CONFIG1["frame"])
+    advance(s, int(g["steps_end"][0]) - CONFIG1["steps"], CONFIG1["converged_frame"])
+    q = s.state()
+    f = s.forces(with_cp=True)
+    s.close()
+    d_rho = density_l2_rel(q[1:N + 1, :, 0], g["rho_end"])
+    d_cp = np.abs(f["Cp"] - g["cp_end"]).max() / np.abs(g["cp_end"]).max()
+    assert d_rho <= TOL_RUN, f"density relative L2 {d_rho:.3e} after {int(g['steps_end'][0])} steps"
+    assert d_cp <= TOL_RUN, f"wall Cp {d_cp:.3e} of max |Cp| after {int(g['steps_end'][0])} steps"
+
+
+@pytest.mark.parametrize("k", range(len(CONFIG2["runs"])), ids=lambda k: CONFIG2["runs"][k]["scheme"])
+def test_config2_runs(k):
+    run = CONFIG2["runs"][k]
+    v = grid(CONFIG2)
+    N = CONFIG2["N"]
+    o = oracle(CONFIG2, v, run)
+    s = solver(CONFIG2, v, run)
+    o.step(1)
+    s.step(1)
+    err1 = normwise(s.state()[1:N + 1], o.state()[1:N + 1])
+    assert err1 <= TOL_STEP1, f"after one step: normwise {err1:.3e}"
+    advance(o, 299, 100)
+    advance(s, 299, 100)
+    ref = o.state()[1:N + 1]
+    q = s.state()[1:N + 1]
+    o.close()
+    s.close()
+    assert np.all(np.isfinite(q))
+    err = normwise(q, ref)
+    assert err <= TOL_RUN, f"after 300 steps: normwise {err:.3e}"

@@ -80,3 +80,30 @@ def test_reference_build_reproduces_fixture(golden):
     r.prepare_state(1)
     r.frame(1)
     assert np.array_equal(r.texture("state2")[1:N + 1], golden[f"{name}/state0"][1:N + 1])
+
+
+@pytest.mark.skipif(not ref_available(), reason="reference shader build not present")
+def test_reference_field_probe(golden):
+    """The field probe of the reference's visualization shader returns the shader's own
+    per-cell quantities: density is state2's rho, temperature p / rho and Mach |v| / a,
+    computed here in float32 in the shader's operation order."""
+    name = "run_slau2_m08_a4_odd"
+    gname, M, N, grid = grid_of(golden, name)
+    r = RefWGSL(M, N)
+    p = params_of(golden, name)
+    r.set_uniforms(p)
+    r.set_grid(grid)
+    r.prepare_state(1)
+    r.frame(2)
+    q = r.texture("state2")[1:N + 1]
+    rho, mx, my, E = (q[..., k] for k in range(4))
+    f32 = np.float32
+    u, v = mx / rho, my / rho
+    pres = (E - f32(0.5) * rho * (u * u + v * v)) * (f32(p.gamma) - f32(1.0))
+    T = pres / rho
+    mach = np.sqrt(u * u + v * v) / np.sqrt(f32(p.gamma) * T)
+    assert np.array_equal(r.field("density"), rho)
+    assert np.array_equal(r.field("pressure"), pres)
+    assert np.array_equal(r.field("temperature"), T)
+    assert np.array_equal(r.field("mach"), mach)
+    r.close()

@@ -6,7 +6,9 @@ avoid an allocation's implicit synchronisation, hosts without a solver handle). 
 hands it device copies of a solver's wall row and body vertices, made here with torch
 (the test may allocate; the entry point does not), and checks Fx, Fy, Cl, Cd and Cp
 against the handle-based ausm_forces on two calls in a row, with the state advanced in
-between.  Tolerance: 1e-4 relative, as the force parity tests.
+between.  Tolerance: 1e-4 relative, as the force parity tests.  The second call must
+also leave the device's free memory unchanged (cudaMemGetInfo, through torch); the first
+call is exempt, because its one-time set-up may load the library's device code.
 """
 import ctypes as C
 import math
@@ -50,10 +52,13 @@ def test_forces_noalloc_matches_forces_twice():
         torch.cuda.synchronize()
         out = np.zeros(6)
         cp = np.zeros(M)
+        free0 = torch.cuda.mem_get_info()[0]
         rc = L.ausm_forces_noalloc(C.c_void_p(wall.data_ptr()), C.c_void_p(body.data_ptr()), M, C.byref(p),
                                    out.ctypes.data_as(C.POINTER(C.c_double)),
                                    cp.ctypes.data_as(C.POINTER(C.c_double)), None)
         assert rc == 0, L.ausm_last_error(None)
+        if call == 1:
+            assert torch.cuda.mem_get_info()[0] == free0, "the call changed the device's free memory"
         scale = math.hypot(ref["Fx"], ref["Fy"])
         assert abs(out[0] - ref["Fx"]) <= TOL * scale and abs(out[1] - ref["Fy"]) <= TOL * scale, call
         cscale = max(abs(ref["Cl"]), abs(ref["Cd"]))
