@@ -50,7 +50,7 @@ METRIC = "Mcell-updates/s per RK3 step"
 # a uniform freestream start, CFL 0.5; seeded.
 BATCH = dict(name="batch64_uneven_128x96-1024x768", count=64, seed=20261203, cells_lo=128 * 96,
              cells_hi=1024 * 768, steps=5000, chunk=100, far_chords=20.0, first_spacing=1e-3, cfl=0.5,
-             grid_iters=200)
+             grid_iters=200, ref_steps=500)
 
 
 def env_rank():
@@ -154,9 +154,11 @@ def build_solver(ausm, wl, engine="fused", M=None, N=None):
 # airfoil (as in BATCH), grid cells log-uniform 16k-1M (aspect 4:3), Mach U[0.3, 6],
 # AoA U[-4, 8] deg, scheme uniform; stop at a 4-decade density-residual drop or 50000
 # steps; admission by a 160 GB HBM budget.  The stream is a bounded sample of
-# `requests` arrivals (the full 10000-request stream is hours of GPU time).
-SERVE = dict(name="served_poisson", seed=20261203, requests=32, rate=200.0, cells_lo=16384, cells_hi=1 << 20,
-             residual_drop=4.0, max_steps=50000, chunk=100, budget=160e9, slots=256, far_chords=20.0,
+# `requests` arrivals (the full 10000-request stream is hours of GPU time) served with
+# `slots` concurrent solves, fewer than the requests, so that requests wait for slots
+# and are admitted as others retire.
+SERVE = dict(name="served_poisson", seed=20261203, requests=48, rate=200.0, cells_lo=16384, cells_hi=1 << 20,
+             residual_drop=4.0, max_steps=50000, chunk=100, budget=160e9, slots=16, far_chords=20.0,
              first_spacing=1e-3, grid_iters=200)
 
 
@@ -203,9 +205,12 @@ def run_served(ausm, cfg, plain):
     srv.stop()
     srv.close()
     lat = np.array([r["latency_ms"] for r in res])
+    queued = np.array([r["queue_ms"] for r in res])
     done = [r for r in res if r["state"] == 0]
     return {"solves_per_s": len(done) / wall, "wall_s": wall, "p50_ms": float(np.percentile(lat, 50)),
-            "p99_ms": float(np.percentile(lat, 99)), "finished": len(done), "failed": len(res) - len(done),
+            "p99_ms": float(np.percentile(lat, 99)), "queue_ms_p50": float(np.percentile(queued, 50)),
+            "queue_ms_max": float(queued.max()), "slots": cfg["slots"] if not plain else 1,
+            "finished": len(done), "failed": len(res) - len(done),
             "converged": sum(1 for r in done if r["stop"] == 1), "max_steps": sum(1 for r in done if r["stop"] == 2),
             "steps_mean": float(np.mean([r["steps"] for r in res])), "rounds": st["rounds"],
             "mcell_updates_per_s": st["cell_updates"] / wall / 1e6, "peak_gb": st["peak_bytes"] / 1e9}, res
@@ -341,6 +346,27 @@ def run_batched(ausm, cfg, warmup, plain=True):
         for a, c in zip(cp_b, cp_p):
             if np.all(np.isfinite(a)) and np.all(np.isfinite(c)):
                 err = max(err, float(np.abs(a - c).max() / max(np.abs(c).max(), 1e-30)))
+    # (c) the plain path as the comparison list of the benchmark configurations defines it:
+    # one solve at a time on the unfused reference-shaped engine (the reference's five
+    # dispatches per stage), timed on a bounded sample of the same run (the first
+    # ref_steps of every solve's steps) and scaled to the full step count
+    ref_plain = None
+    if plain and cfg.get("ref_steps"):
+        rs = cfg["ref_steps"]
+        for s in sols:
+            s.set_engine("reference")
+            s.prepare_state("freestream")
+            s.step(1)
+            s.prepare_state("freestream")
+            s.synchronize()
+        t0 = time.perf_counter()
+        for s in sols:
+            for _ in range(rs // chunk):
+                s.step(chunk, wait=False)
+            s.synchronize()
+        wall_r = (time.perf_counter() - t0) * steps / rs
+        ref_plain = {"engine": "reference-shaped (unfused, 5 dispatches per stage)", "sample_steps": rs,
+                     "wall_s_scaled": wall_r, "solves_per_s": len(sols) / wall_r}
     for s in sols:
         s.close()
     n = len(specs)
@@ -349,6 +375,8 @@ def run_batched(ausm, cfg, warmup, plain=True):
             "device_ms": ms, "wall_s": wall_b, "solves_per_s_wall": n / wall_b,
             "plain_one_launch_per_solve": {"wall_s": wall_p, "solves_per_s": n / wall_p} if plain else None,
             "speedup_vs_plain": wall_p / wall_b if plain else None, "cp_max_rel_diff_vs_plain": err,
+            "plain_reference_shaped": ref_plain,
+            "speedup_vs_plain_reference_shaped": ref_plain["wall_s_scaled"] / wall_b if ref_plain else None,
             "diverged": diverged, "mcell_updates_per_s": cells * steps / (ms * 1e-3) / 1e6,
             "gpu_launches": (3 * chunk * len({sp["scheme"] for sp in specs}) + 3) * (steps // chunk),
             "sizes": f"{min(sp['M'] * sp['N'] for sp in specs)}..{max(sp['M'] * sp['N'] for sp in specs)} cells"}
@@ -490,6 +518,8 @@ def main():
     ap.add_argument("--serve-requests", type=int, default=SERVE["requests"])
     ap.add_argument("--serve-rate", type=float, default=SERVE["rate"])
     ap.add_argument("--serve-max-steps", type=int, default=SERVE["max_steps"])
+    ap.add_argument("--serve-slots", type=int, default=SERVE["slots"])
+    ap.add_argument("--no-serve", action="store_true", help="skip the served stream in --mode step")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched measurement in --mode step")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -517,7 +547,8 @@ def main():
             print(json.dumps(res))
         return 0
     if args.mode == "serve":
-        cfg = dict(SERVE, requests=args.serve_requests, rate=args.serve_rate, max_steps=args.serve_max_steps)
+        cfg = dict(SERVE, requests=args.serve_requests, rate=args.serve_rate, max_steps=args.serve_max_steps,
+                   slots=args.serve_slots)
         res = run_serve_mode(ausm, cfg)
         if rank == 0:
             print(json.dumps(res))
@@ -620,6 +651,13 @@ def main():
         s.close()
         s = None
         batched = run_batched(ausm, BATCH, args.warmup)
+    served = None
+    if world == 1 and not args.no_serve and not args.small:
+        if s is not None:
+            s.close()
+            s = None
+        served = run_serve_mode(ausm, dict(SERVE, requests=args.serve_requests, rate=args.serve_rate,
+                                           max_steps=args.serve_max_steps, slots=args.serve_slots))
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "Mcell-updates/s", "n_gpus": world, "steps": args.steps,
@@ -633,7 +671,7 @@ def main():
                 # per step(1): fused, three stage kernels (dt is computed in stage 1); reference,
                 # 5 dispatches per stage, the dt kernel and the wave-speed reduction
                 "gpu_launches": (3 if args.engine == "fused" else 17) * args.steps, "clocks": clocks, "roofline": roofline, "cpu_baseline": cpu,
-                "e2e": e2e, "batched": batched}
+                "e2e": e2e, "batched": batched, "served": served}
         print(json.dumps(line))
     if s is not None:
         s.close()
