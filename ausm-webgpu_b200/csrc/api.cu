@@ -1003,8 +1003,12 @@ int ausm_synchronize(ausm_solver* h) {
 
 int ausm_debug_set_wait_polls(unsigned polls) {
   NEED(nullptr, polls <= 65536u, AUSM_ERR_INVALID, "polls must be in [0, 65536] (the default bound)");
-  cudaError_t e = set_wait_polls_fused(polls);
+  // the solvers' streams do not synchronise with the copy to the constant: let the work
+  // already queued run with the bound it was queued under, and the next launches see the new one
+  cudaError_t e = cudaDeviceSynchronize();
+  if (e == cudaSuccess) e = set_wait_polls_fused(polls);
   if (e == cudaSuccess) e = set_wait_polls_batch(polls);
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
   if (e != cudaSuccess) return fail(nullptr, AUSM_ERR_CUDA, std::string("wait polls: ") + cudaGetErrorString(e));
   return AUSM_OK;
 }

@@ -197,7 +197,8 @@ int ausm_time_steps(ausm_solver* h, int n, int reps, float* ms_out);
  * current device, in this process.  0 makes every such wait give up at once, so a test
  * can drive the timeout path without a fault: the tiles report AUSM_ERR_TIMEOUT, write
  * nothing, and still let their copies land (second wait, full bound) before they exit.
- * Restore 65536 afterwards. */
+ * The call waits for the device to be idle, so work queued before it keeps the bound it
+ * was queued under.  Restore 65536 afterwards. */
 int ausm_debug_set_wait_polls(unsigned polls);
 /* Tile-height autotuner of the fused engine (no counterpart in the reference): times
  * the TMA stage kernel for tiles of 32 x 8, 32 x 16 and 32 x 32 cells on this solve's
