@@ -161,3 +161,18 @@ def test_body_points_request_matches_naca_request():
     assert ra["state"] == 0 and rb["state"] == 0
     np.testing.assert_array_equal(ra["Cp"], rb["Cp"])
     assert ra["Cl_c"] == ra["Cl"]  # chord 1
+
+
+def test_sharded_server_same_results(alone):
+    """Two servers behind one ShardedServer (both on device 0 here: the placement and
+    routing are what is tested; one server per GPU in production): every request lands
+    on one of them and its result is the same as alone."""
+    import ausm
+    with ausm.ShardedServer([0, 0], 4e9, chunk_steps=CHUNK) as sh:
+        sh.start()
+        ids = [sh.submit(req(k)) for k in range(5)]
+        sh.drain()
+        res = [sh.poll(i) for i in ids]
+    assert {i[0] for i in ids} == {0, 1}
+    for k, d in enumerate(res):
+        same(d, alone[k])
