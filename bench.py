@@ -67,6 +67,16 @@ def max_over_ranks(x: float, dist=None) -> float:
     return float(t.item())
 
 
+def sum_over_ranks(x: float, dist=None) -> float:
+    """Sum of a host scalar over all ranks."""
+    if dist is None or not dist.is_initialized() or dist.get_world_size() == 1:
+        return float(x)
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
 def peaks():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -180,11 +190,23 @@ def serve_stream(cfg):
     return out
 
 
-def run_served(ausm, cfg, plain):
-    """Submits the stream at its arrival times to a server (worker thread) and waits
-    for every result; latency = submit -> result ready."""
-    import numpy as np
+def placed_stream(ausm, cfg, rank, world):
+    """The requests of the stream this rank serves: whole requests placed on devices by
+    budget and work (ausm.place_requests; every rank computes the same placement)."""
     stream = serve_stream(cfg)
+    if world == 1:
+        return stream
+    reqs = [ausm.make_request(sp["M"], sp["N"], naca4=sp["naca"], max_steps=cfg["max_steps"]) for sp in stream]
+    dev = ausm.place_requests([ausm.request_bytes(r) for r in reqs],
+                              [float(r.M) * r.N * r.max_steps for r in reqs], world, cfg["budget"])
+    return [sp for sp, d in zip(stream, dev) if d == rank]
+
+
+def run_served(ausm, cfg, plain, rank=0, world=1):
+    """Submits the stream (this rank's share of it) at its arrival times to a server
+    (worker thread) and waits for every result; latency = submit -> result ready."""
+    import numpy as np
+    stream = placed_stream(ausm, cfg, rank, world)
     srv = ausm.Server(cfg["budget"], cfg["slots"], cfg["chunk"], plain=plain)
     srv.start()
     ids = []
@@ -216,9 +238,16 @@ def run_served(ausm, cfg, plain):
             "mcell_updates_per_s": st["cell_updates"] / wall / 1e6, "peak_gb": st["peak_bytes"] / 1e9}, res
 
 
-def run_serve_mode(ausm, cfg):
-    served, rs = run_served(ausm, cfg, plain=False)
-    plain, rp = run_served(ausm, cfg, plain=True)
+def run_serve_mode(ausm, cfg, rank=0, world=1, dist=None):
+    served, rs = run_served(ausm, cfg, plain=False, rank=rank, world=world)
+    plain, rp = run_served(ausm, cfg, plain=True, rank=rank, world=world)
+    if world > 1:  # whole-job rate: all ranks' solves over the slowest rank's wall time
+        for d in (served, plain):
+            d["rank_wall_s"] = d["wall_s"]
+            d["wall_s"] = max_over_ranks(d["wall_s"], dist)
+            d["finished_rank"] = d["finished"]
+            d["finished"] = int(round(sum_over_ranks(d["finished"], dist)))
+            d["solves_per_s"] = d["finished"] / d["wall_s"]
     err = 0.0
     for a, b in zip(rs, rp):
         if a["state"] == 0 and b["state"] == 0:
@@ -549,7 +578,9 @@ def main():
     if args.mode == "serve":
         cfg = dict(SERVE, requests=args.serve_requests, rate=args.serve_rate, max_steps=args.serve_max_steps,
                    slots=args.serve_slots)
-        res = run_serve_mode(ausm, cfg)
+        res = run_serve_mode(ausm, cfg, rank, world, dist)
+        if world > 1:
+            res["parallelism"] = f"requests placed on {world} GPUs by budget and work, one server each"
         if rank == 0:
             print(json.dumps(res))
         return 0
