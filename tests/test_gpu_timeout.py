@@ -71,8 +71,8 @@ def test_async_step_reports_at_next_wait(polls, reader):
     fn = {"synchronize": s.synchronize, "state": s.state, "forces": lambda: s.forces(with_cp=True),
           "residual_l2": s.residual_l2, "max_wave_speed": s.max_wave_speed}[reader]
     expect_timeout(fn)
-    fn()  # the flag was read and cleared
-    s.prepare_state("freestream")
+    s.prepare_state("freestream")  # the timed-out tiles left the state stale: reset it
+    fn()  # the flag was read and cleared: the same call now succeeds
     assert math.isfinite(s.step(1))
     s.close()
 
