@@ -131,7 +131,7 @@ struct BatchSolve {
   float* dt;
   uint32_t* wave;
   Consts c;
-  int M, N, scheme, tiles_x, tile0, cur;
+  int M, N, scheme, tiles_x, tile0, cur;  // scheme: the work-list group key (scheme, + 4 with MUSCL on)
   int chunk0;  // first residual-norm chunk (512 cells) of the solve
 };
 // Tensor maps per batch member, in this order: halo[0..2], plain[0..2], mi, mj,

@@ -41,7 +41,7 @@ struct ausm_batch {
   std::vector<int> order;
   std::vector<BatchSolve> mirror;  // what the device descriptors hold, in work-list order
   struct Group {
-    int scheme, s_lo, s_hi, t_lo, t_hi;  // descriptors [s_lo, s_hi), work items [t_lo, t_hi)
+    int scheme, s_lo, s_hi, t_lo, t_hi;  // group key (group_key), descriptors [s_lo, s_hi), items [t_lo, t_hi)
   };
   std::vector<Group> groups;
   cudaStream_t aux[2] = {nullptr, nullptr};  // branches of the second and third group
@@ -108,6 +108,10 @@ void drop_graphs(ausm_batch* b) {
   b->graph.clear();
 }
 
+// Work-list group of a member: its scheme, plus 4 when MUSCL is on (the group's
+// kernels are then instantiated with MUSCL known on, without a per-face branch).
+int group_key(const ausm_solver* h) { return h->p.scheme + (h->p.muscl > 0 ? 4 : 0); }
+
 BatchSolve describe(const ausm_solver* h, int tile0, int chunk0, const CUtensorMap* maps) {
   BatchSolve d{};
   d.chunk0 = chunk0;
@@ -120,7 +124,7 @@ BatchSolve describe(const ausm_solver* h, int tile0, int chunk0, const CUtensorM
   d.c = h->c;
   d.M = h->M;
   d.N = h->N;
-  d.scheme = h->p.scheme;
+  d.scheme = group_key(h);
   d.tiles_x = (h->M + kTX - 1) / kTX;
   d.tile0 = tile0;
   d.cur = h->cur;
@@ -187,7 +191,7 @@ void relayout(ausm_batch* b) {
   for (int k = 0; k < n; k++) b->order[k] = k;
   std::stable_sort(b->order.begin(), b->order.end(), [&](int x, int y) {
     const ausm_solver *p = b->members[x], *q = b->members[y];
-    if (p->p.scheme != q->p.scheme) return p->p.scheme < q->p.scheme;
+    if (group_key(p) != group_key(q)) return group_key(p) < group_key(q);
     return (size_t)p->M * p->N > (size_t)q->M * q->N;
   });
   int t = 0;
@@ -201,7 +205,7 @@ void relayout(ausm_batch* b) {
   for (int k : b->order) {
     const ausm_solver* h = b->members[k];
     const int s = (int)b->mirror.size();
-    if (b->groups.empty() || b->groups.back().scheme != h->p.scheme) b->groups.push_back({h->p.scheme, s, s, t, t});
+    if (b->groups.empty() || b->groups.back().scheme != group_key(h)) b->groups.push_back({group_key(h), s, s, t, t});
     b->mirror.push_back(describe(h, t, chunks, maps_of(b, s)));
     const int tx = (h->M + kTX - 1) / kTX, tiles = tx * ((h->N + rows - 1) / rows);
     for (int k = 0; k < tiles; k++) b->items.push_back({s, 0, (k % tx) | (k / tx) << 16, h->M});
@@ -218,7 +222,7 @@ void relayout(ausm_batch* b) {
 // Brings the device descriptors up to date with the members' host state.
 int sync_descriptors(ausm_batch* b) {
   for (size_t k = 0; k < b->members.size(); k++)
-    if (b->members[b->order[k]]->p.scheme != b->mirror[k].scheme) {  // regroup
+    if (group_key(b->members[b->order[k]]) != b->mirror[k].scheme) {  // regroup
       relayout(b);
       break;
     }

@@ -235,9 +235,14 @@ void launch_scheme(int stage, bool emit, const BatchSolve* d, const BatchItem* i
 template <int TY>
 void launch_rows(int scheme, int stage, bool emit, const BatchSolve* d, const BatchItem* items, const int* steps, const CUtensorMap* maps, int t_lo, int t_hi,
                  int rot, int* err, cudaStream_t s) {
-  if (scheme == 0) launch_scheme<0, TY>(stage, emit, d, items, steps, maps, t_lo, t_hi, rot, err, s);
-  else if (scheme == 1) launch_scheme<1, TY>(stage, emit, d, items, steps, maps, t_lo, t_hi, rot, err, s);
-  else launch_scheme<2, TY>(stage, emit, d, items, steps, maps, t_lo, t_hi, rot, err, s);
+  switch (scheme) {  // scheme + 4: MUSCL known on
+    case 0: launch_scheme<0, TY>(stage, emit, d, items, steps, maps, t_lo, t_hi, rot, err, s); break;
+    case 1: launch_scheme<1, TY>(stage, emit, d, items, steps, maps, t_lo, t_hi, rot, err, s); break;
+    case 2: launch_scheme<2, TY>(stage, emit, d, items, steps, maps, t_lo, t_hi, rot, err, s); break;
+    case 4: launch_scheme<4, TY>(stage, emit, d, items, steps, maps, t_lo, t_hi, rot, err, s); break;
+    case 5: launch_scheme<5, TY>(stage, emit, d, items, steps, maps, t_lo, t_hi, rot, err, s); break;
+    default: launch_scheme<6, TY>(stage, emit, d, items, steps, maps, t_lo, t_hi, rot, err, s); break;
+  }
 }
 }  // namespace
 

@@ -135,10 +135,15 @@ void launch_fused_stage(int scheme, int stage, bool emit, const float4* Qs, cons
     else cudaMemsetAsync(wave, 0, sizeof(uint32_t), s);
     dt_mode = 0;
   }
-  switch (scheme) {
+  // TMA stage kernels with MUSCL on are instantiated with it known (scheme + 4)
+  const int sf = scheme + (c.muscl > 0 && tm && stage != 0 ? 4 : 0);
+  switch (sf) {
     case 0: launch_s<0>(stage, emit, Qs, Qn, Qo, Mi, Mj, dt, wave, dt_mode, c, M, N, tm, ty, err, s); break;
     case 1: launch_s<1>(stage, emit, Qs, Qn, Qo, Mi, Mj, dt, wave, dt_mode, c, M, N, tm, ty, err, s); break;
-    default: launch_s<2>(stage, emit, Qs, Qn, Qo, Mi, Mj, dt, wave, dt_mode, c, M, N, tm, ty, err, s); break;
+    case 2: launch_s<2>(stage, emit, Qs, Qn, Qo, Mi, Mj, dt, wave, dt_mode, c, M, N, tm, ty, err, s); break;
+    case 4: launch_s<4>(stage, emit, Qs, Qn, Qo, Mi, Mj, dt, wave, dt_mode, c, M, N, tm, ty, err, s); break;
+    case 5: launch_s<5>(stage, emit, Qs, Qn, Qo, Mi, Mj, dt, wave, dt_mode, c, M, N, tm, ty, err, s); break;
+    default: launch_s<6>(stage, emit, Qs, Qn, Qo, Mi, Mj, dt, wave, dt_mode, c, M, N, tm, ty, err, s); break;
   }
 }
 

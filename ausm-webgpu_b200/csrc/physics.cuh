@@ -323,11 +323,15 @@ __device__ __forceinline__ float4 face_flux(float4 L2, float4 L, float4 R, float
 //    1 / a*^2 from one reciprocal square root (two MUFU operations instead of four);
 //    Mbar^2 = (ML^2 + MR^2) / 2 from the face Mach numbers; the K_p pressure-diffusion
 //    term only when K_p != 0 (uniform per solve; the reference's default is 0).
-template <int SCHEME>
+// SCHEME_FLAGS: the scheme (bits 0-1), plus 4 when the launch knows MUSCL is on, so the
+// kernel has no per-face branch on it (c.muscl is read at run time otherwise).
+template <int SCHEME_FLAGS>
 __device__ __forceinline__ float4 face_flux_len(float4 L2, float4 L, float4 R, float4 R2, float nx, float ny,
                                                 float hl, const Consts& c) {
+  constexpr int SCHEME = SCHEME_FLAGS & 3;
+  constexpr bool MUSCL_ON = (SCHEME_FLAGS & 4) != 0;  // MUSCL known on at compile time
   float4 Lm = L, Rm = R;
-  if (c.muscl > 0) {
+  if (MUSCL_ON || c.muscl > 0) {
     float2 a, b;
     muscl2_packed(lo2(L2), lo2(L), lo2(R), lo2(R2), a, b);
     Lm.x = a.x; Lm.y = a.y; Rm.x = b.x; Rm.y = b.y;

@@ -143,6 +143,16 @@ __device__ __forceinline__ void faces_phase(const float4 (*P)[TX + 4], float4 (*
   if (ty == 0) jface(TY, tx);
 }
 
+// x / 3 correctly rounded (in all but rare halfway cases), as the reference's division:
+// q = x * fl(1/3), then the exact remainder x - 3 q and one correction.  A plain product
+// with fl(1/3) = 1/3 (1 + 3e-8) would scale the whole state by that factor every step,
+// a bias that compounds over thousands of steps.
+__device__ __forceinline__ float2 div3(float2 x) {
+  const float2 t = make_float2(1.0f / 3.0f, 1.0f / 3.0f), m3 = make_float2(-3.0f, -3.0f);
+  const float2 q = mul2(x, t);
+  return fma2(fma2(m3, q, x), t, q);
+}
+
 // Residual and stage combination of the two owned cells from the face fluxes Fi (over
 // Ti) and Fj (over Tj); returns the max wave-speed bits of the new state when EMIT.
 // qn(h) fetches Qn of owned cell h (stages 2, 3).
@@ -179,9 +189,9 @@ __device__ __forceinline__ uint32_t combine_phase(const float4 (*Fi)[TX + 1], co
         o23 = fma2(c75, hi2(n), mul2(c25, fma2(dt2, R23, hi2(q))));
       } else {
         const float4 n = qn(h);
-        const float2 two = make_float2(2.0f, 2.0f), third = make_float2(1.0f / 3.0f, 1.0f / 3.0f);
-        o01 = mul2(fma2(two, fma2(dt2, R01, lo2(q)), lo2(n)), third);
-        o23 = mul2(fma2(two, fma2(dt2, R23, hi2(q)), hi2(n)), third);
+        const float2 two = make_float2(2.0f, 2.0f);
+        o01 = div3(fma2(two, fma2(dt2, R01, lo2(q)), lo2(n)));
+        o23 = div3(fma2(two, fma2(dt2, R23, hi2(q)), hi2(n)));
       }
       const float4 out = make_float4(o01.x, o01.y, o23.x, o23.y);
       Qo[(size_t)j * M + i] = out;

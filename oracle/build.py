@@ -49,9 +49,14 @@ def build_oracle(force: bool = False) -> Path:
     return out
 
 
-def build_ref(force: bool = False) -> Path | None:
-    """Translate and compile the reference's shaders; returns None when the tree is absent."""
-    out = REF_OUT / "libausm_ref.so"
+def build_ref(force: bool = False, contract: bool = False) -> Path | None:
+    """Translate and compile the reference's shaders; returns None when the tree is absent.
+    contract=True builds the same sources with fused multiply-add contraction
+    (-ffp-contract=fast -mfma) into oracle/_ref_fma/: a second float32 rounding of the
+    reference's own arithmetic, used to measure how far two float32 builds of the
+    reference drift apart on a long run."""
+    out_dir = HERE / "_ref_fma" if contract else REF_OUT
+    out = out_dir / "libausm_ref.so"
     if not (REF_SRC / "src" / "shaders" / "ausm.js").exists():
         return out if out.exists() else None
     sys.path.insert(0, str(HERE / "wgsl_ref"))
@@ -61,15 +66,16 @@ def build_ref(force: bool = False) -> Path | None:
     deps += list((REF_SRC / "src").rglob("*.js"))
     if not force and _newer(out, deps):
         return out
-    gen = REF_OUT / "gen"
-    objdir = REF_OUT / "obj"
+    gen = out_dir / "gen"
+    objdir = out_dir / "obj"
     objdir.mkdir(parents=True, exist_ok=True)
     sources = translate.translate_reference(REF_SRC, gen) + [HERE / "wgsl_ref" / "ref_harness.cpp"]
     inc = ["-I", str(HERE / "wgsl_ref"), "-I", str(gen)]
+    flags = [f for f in CXXFLAGS if f != "-ffp-contract=off"] + ["-ffp-contract=fast", "-mfma"] if contract else CXXFLAGS
 
     def compile_one(s: Path):
         o = objdir / (s.stem + ".o")
-        _run(["g++", "-std=c++20", *CXXFLAGS, *inc, "-c", str(s), "-o", str(o)])
+        _run(["g++", "-std=c++20", *flags, *inc, "-c", str(s), "-o", str(o)])
         return o
 
     with cf.ThreadPoolExecutor(max_workers=os.cpu_count() or 4) as ex:

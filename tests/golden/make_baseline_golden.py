@@ -10,6 +10,11 @@ within a test's time:
                       value at the start, or max_steps steps (the served configuration's
                       stopping rule)
   steps_end, l2       step count of the end, residual norms after each frame
+  rho_end_fma,        the same end state from the reference's shaders compiled with fused
+  cp_end_fma          multiply-add contraction (oracle/build.py build_ref(contract=True)): a
+                      second float32 rounding of the reference's own arithmetic, whose
+                      distance from rho_end / cp_end is the float32 reproducibility floor of
+                      this slowly converging subsonic run
   grid_sha256         checksum of the float32 grid (the tests rebuild the grid and check it)
 
 Run where the reference tree is present:
@@ -38,16 +43,19 @@ def residual_l2(r, N):
     return float(np.sqrt(np.mean(res ** 2)))
 
 
-def make():
+def run(grid, lib=None):
+    """The configuration's run on the reference build at `lib` (default: oracle/_ref)."""
+    import oracle.oracle as oo
     c = CONFIG1
     M, N = c["M"], c["N"]
-    grid = make_grid(c)
+    if lib is not None:
+        oo.REF_SO, oo._rlib = lib, None
     r = RefWGSL(M, N)
     r.set_uniforms(make_params(mach=c["mach"], aoa_deg=c["aoa_deg"], scheme=c["scheme"], cfl=c["cfl"]))
     r.set_grid(grid)
     r.prepare_state(1)
     l2 = [residual_l2(r, N)]
-    out = {"grid_sha256": np.array([hashlib.sha256(grid.tobytes()).hexdigest()])}
+    out = {}
     steps = 0
     t0 = time.time()
     while steps < c["steps"]:
@@ -70,6 +78,16 @@ def make():
     out["steps_end"] = np.array([steps])
     out["l2"] = np.array(l2)
     r.close()
+    return out
+
+
+def make():
+    from oracle.build import build_ref
+    grid = make_grid(CONFIG1)
+    out = run(grid)
+    fma = run(grid, build_ref(contract=True))
+    out["rho_end_fma"], out["cp_end_fma"] = fma["rho_end"], fma["cp_end"]
+    out["grid_sha256"] = np.array([hashlib.sha256(grid.tobytes()).hexdigest()])
     path = Path(__file__).resolve().parent / "baseline_c1.npz"
     np.savez_compressed(path, **out)
     return path

@@ -8,8 +8,13 @@ Configuration 1 (NACA 0012, 256 x 128, M 0.5, SLAU2):
     (tests/golden/baseline_c1.npz), density relative L2 and wall Cp (max difference over
     max |Cp|) <= 1e-4 for the fused engine, bit for bit for the reference-shaped engine;
   - the converged run (frames of 500 after that, to a 4-decade density-residual drop or
-    the served configuration's 50000-step limit, whichever comes first; the fixture
-    records where the reference stopped): density L2 and wall Cp within the bound below.
+    the served configuration's 50000-step limit, whichever comes first; the reference
+    stops at the limit, 3.2 decades down): density relative L2 <= 1e-4, and wall Cp
+    within max(1e-4, the spread of the reference itself): the fixture also holds the
+    end state of the reference's shaders compiled with fused multiply-add contraction,
+    and the two float32 builds of the reference differ by 4.2e-4 of max |Cp| there (a
+    slowly converging subsonic mode amplifies round-off), so no float32 code can be held
+    to 1e-4 in Cp at that point; in density they agree to 4.5e-5.
 Configuration 2 (NACA 2412, 512 x 384; M 0.8 SLAU2, M 2 AUSM+-up, M 8 SLAU): one step
   at 1e-5 and 300 steps (frames of 100) at 1e-4 normwise against the float32 oracle run
   on the host cores in the test.
@@ -125,9 +130,12 @@ def test_config1_converged(c1):
     f = s.forces(with_cp=True)
     s.close()
     d_rho = density_l2_rel(q[1:N + 1, :, 0], g["rho_end"])
-    d_cp = np.abs(f["Cp"] - g["cp_end"]).max() / np.abs(g["cp_end"]).max()
+    cmax = np.abs(g["cp_end"]).max()
+    d_cp = np.abs(f["Cp"] - g["cp_end"]).max() / cmax
+    spread = np.abs(g["cp_end_fma"] - g["cp_end"]).max() / cmax  # the reference against itself
     assert d_rho <= TOL_RUN, f"density relative L2 {d_rho:.3e} after {int(g['steps_end'][0])} steps"
-    assert d_cp <= TOL_RUN, f"wall Cp {d_cp:.3e} of max |Cp| after {int(g['steps_end'][0])} steps"
+    assert d_cp <= max(TOL_RUN, spread), \
+        f"wall Cp {d_cp:.3e} of max |Cp| after {int(g['steps_end'][0])} steps (reference spread {spread:.3e})"
 
 
 @pytest.mark.parametrize("k", range(len(CONFIG2["runs"])), ids=lambda k: CONFIG2["runs"][k]["scheme"])
