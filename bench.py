@@ -8,7 +8,11 @@ AoA = 4 deg, SLAU2 + MUSCL, TVD-RK3, CFL 0.5, FP32 state, uniform freestream sta
 (the large precision-study configuration).  Synthetic: the grid and flow are generated
 here, there is no dataset.  One timed step = one TVD-RK3 step (three fused stage
 launches) of the whole grid; the 201 MB state buffers and 403 MB of face records are
-larger than the 126 MB L2, so every step streams them from HBM.
+larger than the 126 MB L2, so every step streams them from HBM.  The timed region (K
+steps, CUDA events on the solver's stream, synchronised on both sides) is repeated for
+about 1.5 s and the median region is reported, with the SM clock sampled by nvidia-smi
+every 50 ms from before the warm-up to the end.  The default line also carries the
+batched configuration (64 uneven grids) and a bounded sample of the served stream.
 
 Multi-GPU (torchrun): every rank advances its own replica of the grid (solves are
 independent; there is no data-path collective), value = all ranks' cell-updates / the
@@ -261,19 +265,28 @@ def run_serve_mode(ausm, cfg, rank=0, world=1, dist=None):
                                            "budget", "slots")}}
 
 
-def run_precision(ausm, steps, chunk=1000):
+def run_precision(ausm, steps, chunk=1000, sensitivity=False):
     """The 4096 x 3072 workload advanced `steps` RK3 steps by the FP32 fused engine
     (FP64 metrics, residual norm and forces) and by the full-FP64 engine from the same
     grid and initial state, dt recomputed every `chunk` steps in both; errors of the
-    FP32 run against the FP64 run."""
+    FP32 run against the FP64 run (both start from the float32 freestream, the FP64 engine
+    from it widened).  sensitivity: a second FP64 run from the freestream in double (1e-8
+    away from the float32 one): how far two FP64 runs drift apart from that alone, the
+    floor for any float32 run of this flow."""
     import numpy as np
     wl = dict(WORKLOAD)
     out = {"metric": "precision study", "workload": wl["name"], "steps": steps, "chunk": chunk}
     runs = {}
-    for engine in ("fused", "f64"):
+    centres = None
+    for engine in ("fused", "f64") + (("f64_exact_start",) if sensitivity else ()):
         s = build_solver(ausm, wl)
+        if centres is None:
+            v = s.vertices().astype(np.float64)
+            centres = 0.25 * (v[:-1] + np.roll(v[:-1], -1, axis=1) + v[1:] + np.roll(v[1:], -1, axis=1))
         if engine != "fused":
-            s.set_engine(engine)
+            s.set_engine("f64")  # carries the float32 freestream over, widened
+            if engine == "f64_exact_start":
+                s.prepare_state("freestream")  # the freestream in double
         t0 = time.perf_counter()
         done = 0
         while done < steps:
@@ -290,6 +303,12 @@ def run_precision(ausm, steps, chunk=1000):
         return rho, p
     r32, p32 = prim(runs["fused"]["q"])
     r64, p64 = prim(runs["f64"]["q"])
+    # where the density differs by more than 1e-2 of its max: downstream of the trailing
+    # edge (x > 0.5 chord) or not, and the radius of those cells
+    big = np.abs(r32 - r64) > 1e-2 * np.abs(r64).max()
+    rad = np.hypot(centres[..., 0], centres[..., 1])
+    out["rho_1e-2_cells"] = {"count": int(big.sum()), "downstream_fraction": float((centres[..., 0][big] > 0.5).mean())
+                             if big.any() else None, "radius_median": float(np.median(rad[big])) if big.any() else None}
     def errs(a, b):
         out = {"max_rel": float(np.abs(a - b).max() / np.abs(b).max()),
                "l2_rel": float(np.sqrt(np.mean((a - b) ** 2)) / np.sqrt(np.mean(b ** 2)))}
@@ -311,6 +330,12 @@ def run_precision(ausm, steps, chunk=1000):
                 "cd": {"f32": F32["Cd"], "f64": F64["Cd"], "rel": abs(F32["Cd"] - F64["Cd"]) / abs(F64["Cd"])},
                 "residual_l2": {"f32": runs["fused"]["l2"], "f64": runs["f64"]["l2"]},
                 "seconds": {"f32": runs["fused"]["seconds"], "f64": runs["f64"]["seconds"]}})
+    if sensitivity:
+        rb, pb = prim(runs["f64_exact_start"]["q"])
+        Fb = runs["f64_exact_start"]["F"]
+        out["f64_exact_start_vs_f64"] = {
+            "rho": errs(rb, r64), "p": errs(pb, p64), "cp": errs(Fb["Cp"], cp64),
+            "cl_rel": abs(Fb["Cl"] - F64["Cl"]) / abs(F64["Cl"]), "cd_rel": abs(Fb["Cd"] - F64["Cd"]) / abs(F64["Cd"])}
     return out
 
 
@@ -547,11 +572,14 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--small", action="store_true", help="512x384 grid (profiling and quick checks)")
+    ap.add_argument("--grid", default=None, help="MxN grid of the same flow instead of 4096x3072 (profiling cases)")
     ap.add_argument("--mode", default="step", choices=["step", "batch", "serve", "precision"],
                     help="step: the 4096x3072 step (headline line, with the batched measurement "
                          "attached); batch: the batched measurement alone; serve: the served stream; "
                          "precision: FP32 against FP64 on the 4096x3072 workload")
     ap.add_argument("--precision-steps", type=int, default=100000)
+    ap.add_argument("--precision-sensitivity", action="store_true",
+                    help="also an FP64 run from the freestream in double (sensitivity of the flow)")
     ap.add_argument("--batch-steps", type=int, default=BATCH["steps"],
                     help="steps per solve of the batched measurement (shorter runs for profiling only)")
     ap.add_argument("--no-plain", action="store_true", help="batched measurement without the plain comparison")
@@ -582,7 +610,7 @@ def main():
             print(json.dumps(res))
         return 0
     if args.mode == "precision":
-        res = run_precision(ausm, args.precision_steps)
+        res = run_precision(ausm, args.precision_steps, sensitivity=args.precision_sensitivity)
         if rank == 0:
             print(json.dumps(res))
         return 0
@@ -598,6 +626,9 @@ def main():
     wl = dict(WORKLOAD)
     if args.small:
         wl.update(M=512, N=384, name="naca0024_512x384_m6_aoa4_slau2")
+    if args.grid:
+        gm, gn = (int(x) for x in args.grid.lower().split("x"))
+        wl.update(M=gm, N=gn, name=f"naca0024_{gm}x{gn}_m6_aoa4_slau2")
     s = build_solver(ausm, wl, engine=args.engine)
     M, N = s.M, s.N
     cells = M * N
