@@ -265,25 +265,29 @@ def run_serve_mode(ausm, cfg, rank=0, world=1, dist=None):
                                            "budget", "slots")}}
 
 
-def run_precision(ausm, steps, chunk=1000, sensitivity=False):
+def run_precision(ausm, steps, chunk=1000, sensitivity=False, reference=False):
     """The 4096 x 3072 workload advanced `steps` RK3 steps by the FP32 fused engine
     (FP64 metrics, residual norm and forces) and by the full-FP64 engine from the same
     grid and initial state, dt recomputed every `chunk` steps in both; errors of the
     FP32 run against the FP64 run (both start from the float32 freestream, the FP64 engine
     from it widened).  sensitivity: a second FP64 run from the freestream in double (1e-8
     away from the float32 one): how far two FP64 runs drift apart from that alone, the
-    floor for any float32 run of this flow."""
+    floor for any float32 run of this flow.  reference: the reference-shaped FP32 engine
+    (the reference's arithmetic bit for bit, FP32 metrics) against the FP64 run too."""
     import numpy as np
     wl = dict(WORKLOAD)
     out = {"metric": "precision study", "workload": wl["name"], "steps": steps, "chunk": chunk}
     runs = {}
     centres = None
-    for engine in ("fused", "f64") + (("f64_exact_start",) if sensitivity else ()):
+    for engine in (("fused", "f64") + (("f64_exact_start",) if sensitivity else ())
+                   + (("reference",) if reference else ())):
         s = build_solver(ausm, wl)
         if centres is None:
             v = s.vertices().astype(np.float64)
             centres = 0.25 * (v[:-1] + np.roll(v[:-1], -1, axis=1) + v[1:] + np.roll(v[1:], -1, axis=1))
-        if engine != "fused":
+        if engine == "reference":
+            s.set_engine("reference")
+        elif engine != "fused":
             s.set_engine("f64")  # carries the float32 freestream over, widened
             if engine == "f64_exact_start":
                 s.prepare_state("freestream")  # the freestream in double
@@ -308,7 +312,10 @@ def run_precision(ausm, steps, chunk=1000, sensitivity=False):
     big = np.abs(r32 - r64) > 1e-2 * np.abs(r64).max()
     rad = np.hypot(centres[..., 0], centres[..., 1])
     out["rho_1e-2_cells"] = {"count": int(big.sum()), "downstream_fraction": float((centres[..., 0][big] > 0.5).mean())
-                             if big.any() else None, "radius_median": float(np.median(rad[big])) if big.any() else None}
+                             if big.any() else None, "radius_median": float(np.median(rad[big])) if big.any() else None,
+                             "x_range": [float(centres[..., 0][big].min()), float(centres[..., 0][big].max())]
+                             if big.any() else None,
+                             "j_range": [int(np.nonzero(big)[0].min()), int(np.nonzero(big)[0].max())] if big.any() else None}
     def errs(a, b):
         out = {"max_rel": float(np.abs(a - b).max() / np.abs(b).max()),
                "l2_rel": float(np.sqrt(np.mean((a - b) ** 2)) / np.sqrt(np.mean(b ** 2)))}
@@ -330,6 +337,14 @@ def run_precision(ausm, steps, chunk=1000, sensitivity=False):
                 "cd": {"f32": F32["Cd"], "f64": F64["Cd"], "rel": abs(F32["Cd"] - F64["Cd"]) / abs(F64["Cd"])},
                 "residual_l2": {"f32": runs["fused"]["l2"], "f64": runs["f64"]["l2"]},
                 "seconds": {"f32": runs["fused"]["seconds"], "f64": runs["f64"]["seconds"]}})
+    if reference:
+        rr, pr = prim(runs["reference"]["q"])
+        Fr = runs["reference"]["F"]
+        big = np.abs(rr - r64) > 1e-2 * np.abs(r64).max()
+        out["reference_vs_f64"] = {
+            "rho": errs(rr, r64), "p": errs(pr, p64), "cp": errs(Fr["Cp"], cp64),
+            "cl_rel": abs(Fr["Cl"] - F64["Cl"]) / abs(F64["Cl"]), "cd_rel": abs(Fr["Cd"] - F64["Cd"]) / abs(F64["Cd"]),
+            "rho_1e-2_cells": int(big.sum()), "seconds": runs["reference"]["seconds"]}
     if sensitivity:
         rb, pb = prim(runs["f64_exact_start"]["q"])
         Fb = runs["f64_exact_start"]["F"]
@@ -578,6 +593,8 @@ def main():
                          "attached); batch: the batched measurement alone; serve: the served stream; "
                          "precision: FP32 against FP64 on the 4096x3072 workload")
     ap.add_argument("--precision-steps", type=int, default=100000)
+    ap.add_argument("--precision-reference", action="store_true",
+                    help="also the reference-shaped FP32 engine against FP64")
     ap.add_argument("--precision-sensitivity", action="store_true",
                     help="also an FP64 run from the freestream in double (sensitivity of the flow)")
     ap.add_argument("--batch-steps", type=int, default=BATCH["steps"],
@@ -610,7 +627,8 @@ def main():
             print(json.dumps(res))
         return 0
     if args.mode == "precision":
-        res = run_precision(ausm, args.precision_steps, sensitivity=args.precision_sensitivity)
+        res = run_precision(ausm, args.precision_steps, sensitivity=args.precision_sensitivity,
+                            reference=args.precision_reference)
         if rank == 0:
             print(json.dumps(res))
         return 0
