@@ -265,7 +265,7 @@ def run_serve_mode(ausm, cfg, rank=0, world=1, dist=None):
                                            "budget", "slots")}}
 
 
-def run_precision(ausm, steps, chunk=1000, sensitivity=False, reference=False):
+def run_precision(ausm, steps, chunk=1000, sensitivity=False, reference=False, noise=False):
     """The 4096 x 3072 workload advanced `steps` RK3 steps by the FP32 fused engine
     (FP64 metrics, residual norm and forces) and by the full-FP64 engine from the same
     grid and initial state, dt recomputed every `chunk` steps in both; errors of the
@@ -273,14 +273,17 @@ def run_precision(ausm, steps, chunk=1000, sensitivity=False, reference=False):
     from it widened).  sensitivity: a second FP64 run from the freestream in double (1e-8
     away from the float32 one): how far two FP64 runs drift apart from that alone, the
     floor for any float32 run of this flow.  reference: the reference-shaped FP32 engine
-    (the reference's arithmetic bit for bit, FP32 metrics) against the FP64 run too."""
+    (the reference's arithmetic bit for bit, FP32 metrics) against the FP64 run too.
+    noise: an FP64 run from the float32 start with each cell's state changed by about one
+    float32 rounding (relative N(0, 1e-7), seeded): how far round-off-sized per-cell noise
+    alone takes an FP64 run."""
     import numpy as np
     wl = dict(WORKLOAD)
     out = {"metric": "precision study", "workload": wl["name"], "steps": steps, "chunk": chunk}
     runs = {}
     centres = None
     for engine in (("fused", "f64") + (("f64_exact_start",) if sensitivity else ())
-                   + (("reference",) if reference else ())):
+                   + (("reference",) if reference else ()) + (("f64_noisy_start",) if noise else ())):
         s = build_solver(ausm, wl)
         if centres is None:
             v = s.vertices().astype(np.float64)
@@ -291,6 +294,11 @@ def run_precision(ausm, steps, chunk=1000, sensitivity=False, reference=False):
             s.set_engine("f64")  # carries the float32 freestream over, widened
             if engine == "f64_exact_start":
                 s.prepare_state("freestream")  # the freestream in double
+            if engine == "f64_noisy_start":
+                q = s.state()
+                rng = np.random.default_rng(7)
+                q[1:s.N + 1] *= (1.0 + 1e-7 * rng.standard_normal(q[1:s.N + 1].shape)).astype(np.float32)
+                s.set_state(q)
         t0 = time.perf_counter()
         done = 0
         while done < steps:
@@ -345,6 +353,13 @@ def run_precision(ausm, steps, chunk=1000, sensitivity=False, reference=False):
             "rho": errs(rr, r64), "p": errs(pr, p64), "cp": errs(Fr["Cp"], cp64),
             "cl_rel": abs(Fr["Cl"] - F64["Cl"]) / abs(F64["Cl"]), "cd_rel": abs(Fr["Cd"] - F64["Cd"]) / abs(F64["Cd"]),
             "rho_1e-2_cells": int(big.sum()), "seconds": runs["reference"]["seconds"]}
+    if noise:
+        rn, pn = prim(runs["f64_noisy_start"]["q"])
+        Fn = runs["f64_noisy_start"]["F"]
+        out["f64_noisy_start_vs_f64"] = {
+            "rho": errs(rn, r64), "p": errs(pn, p64), "cp": errs(Fn["Cp"], cp64),
+            "cl_rel": abs(Fn["Cl"] - F64["Cl"]) / abs(F64["Cl"]), "cd_rel": abs(Fn["Cd"] - F64["Cd"]) / abs(F64["Cd"]),
+            "rho_1e-2_cells": int(np.count_nonzero(np.abs(rn - r64) > 1e-2 * np.abs(r64).max()))}
     if sensitivity:
         rb, pb = prim(runs["f64_exact_start"]["q"])
         Fb = runs["f64_exact_start"]["F"]
@@ -593,6 +608,8 @@ def main():
                          "attached); batch: the batched measurement alone; serve: the served stream; "
                          "precision: FP32 against FP64 on the 4096x3072 workload")
     ap.add_argument("--precision-steps", type=int, default=100000)
+    ap.add_argument("--precision-noise", action="store_true",
+                    help="also an FP64 run from a start with round-off-sized per-cell noise")
     ap.add_argument("--precision-reference", action="store_true",
                     help="also the reference-shaped FP32 engine against FP64")
     ap.add_argument("--precision-sensitivity", action="store_true",
@@ -628,7 +645,7 @@ def main():
         return 0
     if args.mode == "precision":
         res = run_precision(ausm, args.precision_steps, sensitivity=args.precision_sensitivity,
-                            reference=args.precision_reference)
+                            reference=args.precision_reference, noise=args.precision_noise)
         if rank == 0:
             print(json.dumps(res))
         return 0
