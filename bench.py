@@ -8,9 +8,12 @@ AoA = 4 deg, SLAU2 + MUSCL, TVD-RK3, CFL 0.5, FP32 state, uniform freestream sta
 (the large precision-study configuration).  Synthetic: the grid and flow are generated
 here, there is no dataset.  One timed step = one TVD-RK3 step (three fused stage
 launches) of the whole grid; the 201 MB state buffers and 403 MB of face records are
-larger than the 126 MB L2, so every step streams them from HBM.  The timed region (K
-steps, CUDA events on the solver's stream, synchronised on both sides) is repeated for
-about 1.5 s and the median region is reported, with the SM clock sampled by nvidia-smi
+larger than the 126 MB L2, so every step streams them from HBM.  The timed region is
+one reference frame of K steps (step(K): dt from the state at the frame's start, one CFL
+reduction at its end, main.js:744-791), CUDA events on the solver's stream, synchronised
+on both sides; it is repeated for about 1.5 s and the median region is reported (regions
+of K separate step(1) calls, dt every step, alternate with them and are reported
+beside as ms_per_step_dt_every_step), with the SM clock sampled by nvidia-smi
 every 50 ms from before the warm-up to the end.  The default line also carries the
 batched configuration (64 uneven grids) and a bounded sample of the served stream.
 
@@ -672,22 +675,30 @@ def main():
     # timed region (K steps, CUDA events on the solver's stream, synchronised, barrier
     # first) is repeated until about TIMED_S seconds have passed, so that the clock record
     # covers it; the median region counts.  Every rank repeats it the same number of times.
+    # A timed region is one reference frame of K steps, step(K): dt from the state at its
+    # start, held for the K steps, and one CFL wave-speed reduction at its end, as the
+    # reference's frame loop (main.js:744-791).  Regions of K separate step(1) calls (dt
+    # and the reduction every step) alternate with them and are reported beside.
     with Clocks(local_rank) as clk:
         for _ in range(args.warmup):
             s.step(1, wait=False)
         s.synchronize()
-        probe = s.time_steps(1, args.steps)
+        probe = s.time_steps(args.steps, 1)
         reps = int(max_over_ranks(max(3, min(500, math.ceil(TIMED_S * 1e3 / max(probe, 1e-3)))), dist))
-        times, walls = [], []
+        times, walls, times_each = [], [], []
         for _ in range(reps):
             if dist:
                 dist.barrier()
             t0 = time.perf_counter()
-            times.append(s.time_steps(1, args.steps))
+            times.append(s.time_steps(args.steps, 1))
             walls.append(time.perf_counter() - t0)
+            if dist:
+                dist.barrier()
+            times_each.append(s.time_steps(1, args.steps))
     clocks = clk.summary()
     dt_check = s.step(0)  # raises if the run diverged
     ms_med = statistics.median(times)
+    ms_each = max_over_ranks(statistics.median(times_each), dist)
     ms = max_over_ranks(ms_med, dist)
     wall = statistics.median(walls)
     value = world * cells * args.steps / (ms * 1e-3) / 1e6
@@ -775,10 +786,12 @@ def main():
                            "parallelism": f"replicas{world}", "l2": ("inputs larger than L2" if cells * 16 > 126e6 else "inputs fit in L2") +
                            f" ({cells * 16 / 1e6:.0f} MB state, {cells * 32 / 1e6:.0f} MB face records)",
                            "wall_s": wall, "timed_regions": len(times),
-                           "ms_per_step_min_max": [min(times) / args.steps, max(times) / args.steps]},
+                           "ms_per_step_min_max": [min(times) / args.steps, max(times) / args.steps],
+                           "timed_region": f"one frame of {args.steps} steps (dt held, one CFL reduction)",
+                           "ms_per_step_dt_every_step": ms_each / args.steps},
                 # per step(1): fused, three stage kernels (dt is computed in stage 1); reference,
                 # 5 dispatches per stage, the dt kernel and the wave-speed reduction
-                "gpu_launches": (3 if args.engine == "fused" else 17) * args.steps, "clocks": clocks, "roofline": roofline, "cpu_baseline": cpu,
+                "gpu_launches": 3 * args.steps if args.engine == "fused" else 15 * args.steps + 3, "clocks": clocks, "roofline": roofline, "cpu_baseline": cpu,
                 "e2e": e2e, "batched": batched, "served": served}
         print(json.dumps(line))
     if s is not None:

@@ -93,8 +93,16 @@ def test_forces_and_residual(golden, name, engine):
     assert f["Cp"].shape == (M,) and np.all(np.isfinite(f["Cp"]))
     r_ref = golden[f"{name}/residual"][..., 0].astype(np.float64)
     l2_ref = math.sqrt(np.mean(r_ref ** 2))
+    # after the frames: the fused engine's state is within 1e-4 of the reference's, and
+    # the residual (a difference of nearly cancelling fluxes) of a state that far off
+    # differs by up to 1e-3 of its norm; on the reference's own state (below) the
+    # residual evaluation itself is held to 2e-5
     tol = 0.0 if engine == "reference" else 1e-3
     assert abs(s.residual_l2() - l2_ref) <= tol * l2_ref + 1e-12
+    k = len(golden[f"{name}/frames"]) - 1
+    s.set_state(golden[f"{name}/state{k}"])
+    tol_same = 0.0 if engine == "reference" else 2e-5
+    assert abs(s.residual_l2() - l2_ref) <= tol_same * l2_ref + 1e-12
     s.close()
 
 
