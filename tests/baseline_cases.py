@@ -21,8 +21,7 @@ import math
 import numpy as np
 
 CONFIG1 = dict(M=256, N=128, naca=12, far=20.0, first=1e-3, iters=2000, mach=0.5, aoa_deg=0.0, scheme="SLAU2",
-               cfl=0.5, steps=2000, frame=100, converged_frame=500, max_steps=50000, drop=4.0,
-               conv_max_steps=300000)
+               cfl=0.5, steps=2000, frame=100, converged_frame=500, max_steps=50000, drop=4.0)
 CONFIG2 = dict(M=512, N=384, naca=2412, far=20.0, first=1e-3, iters=2000, cfl=0.5,
                runs=[dict(mach=0.8, aoa_deg=2.0, scheme="SLAU2"), dict(mach=2.0, aoa_deg=0.0, scheme="AUSM+-up"),
                      dict(mach=8.0, aoa_deg=0.0, scheme="SLAU")])
