@@ -101,7 +101,11 @@ def stretched_guess(body, outer, N: int, first_spacing: float) -> np.ndarray:
                 lo, hi = 1e-6, 1.0 - 1e-12
             for _ in range(200):
                 q = 0.5 * (lo + hi)
-                sN = h * (math.pow(q, N) - 1.0) / (q - 1.0)
+                try:
+                    qN = math.pow(q, N)
+                except OverflowError:  # q^N beyond double: infinite, as pow returns in C
+                    qN = math.inf
+                sN = h * (qN - 1.0) / (q - 1.0)
                 if (sN > 1.0) == (h * N < 1.0):
                     hi = q
                 else:
