@@ -260,6 +260,26 @@ void retire(ausm_server* s, Req* q, int stop) {
   finish(s, q, state, stop);
 }
 
+// A failed round: its batch members end with the round's status (a timed-out tile, a
+// CUDA error); queued requests stay queued (a broken device fails them at their own
+// admission).  Returns the status, as the round does.
+int fail_round(ausm_server* s, const std::vector<Req*>& act, int rc, const std::string& why) {
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    for (Req* q : act)
+      for (size_t k = 0; k < s->active.size(); k++)
+        if (s->active[k] == q) {
+          s->active.erase(s->active.begin() + k);
+          break;
+        }
+  }
+  for (Req* q : act) {
+    q->err = why;
+    finish(s, q, rc, 0);
+  }
+  return sfail(s, rc, why);
+}
+
 int pump_round(ausm_server* s, int* remaining) {
   std::lock_guard<std::mutex> pl(s->pump_mu);
   if (s->dev < 0) {
@@ -336,9 +356,9 @@ int pump_round(ausm_server* s, int* remaining) {
       }
     } else {
       int rc = ausm_batch_step(s->batch, s->chunk, dtw.data());
-      if (rc != AUSM_OK && rc != AUSM_ERR_DIVERGED) return sfail(s, rc, ausm_batch_last_error(s->batch));
+      if (rc != AUSM_OK && rc != AUSM_ERR_DIVERGED) return fail_round(s, act, rc, ausm_batch_last_error(s->batch));
       rc = ausm_batch_residual_l2(s->batch, l2.data());
-      if (rc != AUSM_OK) return sfail(s, rc, ausm_batch_last_error(s->batch));
+      if (rc != AUSM_OK) return fail_round(s, act, rc, ausm_batch_last_error(s->batch));
     }
     std::vector<std::pair<Req*, int>> done;
     {
@@ -386,22 +406,7 @@ void worker_loop(ausm_server* s) {
       if (s->stopping) return;
     }
     int left = 0;
-    const int rc = pump_round(s, &left);
-    if (rc != AUSM_OK) {
-      // a round failed: its batch members end with the round's status; queued requests
-      // stay queued (a broken device fails them at their own admission)
-      std::vector<Req*> act;
-      std::string why;
-      {
-        std::lock_guard<std::mutex> lk(s->mu);
-        act.assign(s->active.begin(), s->active.end());
-        s->active.clear();
-        why = s->err;
-      }
-      for (Req* q : act) {
-        q->err = why;
-        finish(s, q, rc, 0);
-      }
+    if (pump_round(s, &left) != AUSM_OK) {  // the round's members were ended by fail_round
       std::lock_guard<std::mutex> lk(s->mu);
       s->cv.notify_all();
     }

@@ -176,3 +176,25 @@ def test_sharded_server_same_results(alone):
     assert {i[0] for i in ids} == {0, 1}
     for k, d in enumerate(res):
         same(d, alone[k])
+
+
+def test_failed_round_ends_only_its_members(alone):
+    """A round whose batch step fails (here a bounded tile wait made to give up at once
+    through the test hook, no fault) ends the requests of that round with its status;
+    a request still queued behind them is served afterwards with its usual result."""
+    import ausm
+    from ausm import _lib
+    with ausm.Server(4e9, max_active=1, chunk_steps=CHUNK) as s:
+        a, b = s.submit(req(0)), s.submit(req(1))
+        s.pump()  # admits a (one slot) and runs its first round
+        ausm.set_wait_polls(0)
+        try:
+            with pytest.raises(ausm.AusmError) as e:
+                s.pump()
+            assert e.value.code == _lib.ERR_TIMEOUT
+        finally:
+            ausm.set_wait_polls(65536)
+        assert s.poll(a)["state"] == _lib.ERR_TIMEOUT
+        assert s.poll(b)["state"] == _lib.REQ_QUEUED
+        s.drain()
+        same(s.poll(b), alone[1])
