@@ -158,3 +158,35 @@ def test_config2_runs(k):
     assert np.all(np.isfinite(q))
     err = normwise(q, ref)
     assert err <= TOL_RUN, f"after 300 steps: normwise {err:.3e}"
+
+
+GOLDEN_C2 = Path(__file__).resolve().parent / "golden" / "baseline_c2.npz"
+
+
+@pytest.mark.skipif(not GOLDEN_C2.exists(), reason="configuration-2 fixture not generated")
+@pytest.mark.parametrize("k", range(len(CONFIG2["runs"])), ids=lambda k: CONFIG2["runs"][k]["scheme"])
+def test_config2_as_written(k):
+    """Configuration 2 as written: 20000 RK3 steps in frames of 100 against the
+    reference's own shaders (tests/golden/baseline_c2.npz).  Density (relative L2 over
+    every 4th cell in i and j) and wall Cp (max over max |Cp|) within max(1e-4, the
+    spread between the reference and the same shaders compiled with FMA contraction)."""
+    g = dict(np.load(GOLDEN_C2))
+    run = CONFIG2["runs"][k]
+    v = grid(CONFIG2)
+    assert hashlib.sha256(v.tobytes()).hexdigest() == str(g["grid_sha256"][0])
+    N = CONFIG2["N"]
+    s = solver(CONFIG2, v, run)
+    advance(s, 20000, 100)
+    q = s.state()
+    f = s.forces(with_cp=True)
+    s.close()
+    assert np.all(np.isfinite(q))
+    rho = q[1:N + 1:4, ::4, 0]
+    ref_rho, ref_cp = g[f"{k}/rho_sub"], g[f"{k}/cp"]
+    d_rho = density_l2_rel(rho, ref_rho)
+    s_rho = density_l2_rel(g[f"{k}/rho_sub_fma"], ref_rho)
+    cmax = np.abs(ref_cp).max()
+    d_cp = np.abs(f["Cp"] - ref_cp).max() / cmax
+    s_cp = np.abs(g[f"{k}/cp_fma"] - ref_cp).max() / cmax
+    assert d_rho <= max(TOL_RUN, s_rho), f"density relative L2 {d_rho:.3e} (reference spread {s_rho:.3e})"
+    assert d_cp <= max(TOL_RUN, s_cp), f"wall Cp {d_cp:.3e} of max |Cp| (reference spread {s_cp:.3e})"
