@@ -40,12 +40,17 @@ def _newer(out: Path, deps) -> bool:
     return all(Path(d).stat().st_mtime <= t for d in deps)
 
 
-def build_oracle(force: bool = False) -> Path:
-    BUILD.mkdir(exist_ok=True)
-    out = BUILD / "libausm_oracle.so"
+def build_oracle(force: bool = False, contract: bool = False) -> Path:
+    """The restatement; contract=True builds it with fused multiply-add contraction
+    (-ffp-contract=fast -mfma) into oracle/_build_fma/, a second float32 rounding of the
+    same arithmetic (for the float32 spread of long runs)."""
+    out_dir = HERE / "_build_fma" if contract else BUILD
+    out_dir.mkdir(exist_ok=True)
+    out = out_dir / "libausm_oracle.so"
     src = HERE / "ausm_oracle.cpp"
+    flags = [f for f in CXXFLAGS if f != "-ffp-contract=off"] + ["-ffp-contract=fast", "-mfma"] if contract else CXXFLAGS
     if force or not _newer(out, [src, __file__]):
-        _run(["g++", "-std=c++17", *CXXFLAGS, "-shared", str(src), "-o", str(out)])
+        _run(["g++", "-std=c++17", *flags, "-shared", str(src), "-o", str(out)])
     return out
 
 

@@ -166,10 +166,11 @@ GOLDEN_C2 = Path(__file__).resolve().parent / "golden" / "baseline_c2.npz"
 @pytest.mark.skipif(not GOLDEN_C2.exists(), reason="configuration-2 fixture not generated")
 @pytest.mark.parametrize("k", range(len(CONFIG2["runs"])), ids=lambda k: CONFIG2["runs"][k]["scheme"])
 def test_config2_as_written(k):
-    """Configuration 2 as written: 20000 RK3 steps in frames of 100 against the
-    reference's own shaders (tests/golden/baseline_c2.npz).  Density (relative L2 over
-    every 4th cell in i and j) and wall Cp (max over max |Cp|) within max(1e-4, the
-    spread between the reference and the same shaders compiled with FMA contraction)."""
+    """Configuration 2 as written: 20000 RK3 steps in frames of 100 against the float32
+    oracle, which reproduces the reference's shaders bit for bit (tests/golden/
+    baseline_c2.npz).  Density (relative L2 over every 4th cell in i and j) and wall Cp
+    (max over max |Cp|) within max(1e-4, the spread between the oracle and the same
+    oracle compiled with FMA contraction)."""
     g = dict(np.load(GOLDEN_C2))
     run = CONFIG2["runs"][k]
     v = grid(CONFIG2)
