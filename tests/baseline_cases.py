@@ -63,3 +63,36 @@ def density_l2_rel(a, b):
     a = np.asarray(a, np.float64)
     b = np.asarray(b, np.float64)
     return float(np.sqrt(np.mean((a - b) ** 2)) / np.sqrt(np.mean(b ** 2)))
+
+
+# Configuration 5 ("large precision study": NACA 0024, far field at 40 chords, M 6, AoA 4,
+# SLAU2 + MUSCL, CFL 0.5) on the 1024 x 768 sub-grid where the FP64 oracle runs on the
+# host cores: the grid of the 4096 x 3072 workload's generator at that size (geometric
+# stretch with a 1e-3 chord first cell, 200 multicolour TTM sweeps in double, rounded to
+# float32), dt recomputed every 1000 steps as in the full-size precision study.
+CONFIG5_SUB = dict(M=1024, N=768, naca=24, far=40.0, first=1e-3, iters=200, mach=6.0, aoa_deg=4.0, scheme="SLAU2",
+                   cfl=0.5, chunk=1000, checkpoints=(2000, 20000, 100000), sub=8)
+
+
+def make_grid_multicolor(cfg):
+    """float32 (N+1, M, 2) vertices: the stretched guess, then cfg['iters'] multicolour
+    sweeps of the oracle's FP64 restatement of the library's generator."""
+    from oracle.geometry_ref import circular_outer, naca4_boundary, stretched_guess
+    from oracle.oracle import Oracle
+    M, N = cfg["M"], cfg["N"]
+    body = naca4_boundary(M, cfg["naca"], 0.5, 0.0)
+    outer = circular_outer(M, cfg["far"])
+    o = Oracle(M, N, "f64")
+    o.set_vertices(stretched_guess(body, outer, N, cfg["first"]))
+    o.grid_multicolor(cfg["iters"], 0.0)
+    v = o.vertices().astype(np.float32)
+    o.close()
+    return v
+
+
+def primitives(q, gamma=1.4):
+    """density and pressure (float64) of conserved states (..., 4)"""
+    q = np.asarray(q, np.float64)
+    rho = q[..., 0]
+    p = (q[..., 3] - 0.5 * (q[..., 1] ** 2 + q[..., 2] ** 2) / rho) * (gamma - 1.0)
+    return rho, p
