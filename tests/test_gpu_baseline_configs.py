@@ -207,31 +207,36 @@ C5_ENGINES = {}
 
 def c5_run(v, engine):
     """Configuration 5's flow on the 1024 x 768 sub-grid by one engine, dt recomputed every
-    1000 steps, observed at the fixture's checkpoints (run once per engine per module)."""
+    1000 steps, observed at the fixture's checkpoints, with the lift and drag after every
+    1000 steps (run once per engine per module)."""
     from ausm import Solver
     if engine in C5_ENGINES:
         return C5_ENGINES[engine]
     cfg = CONFIG5_SUB
-    M, N, sub = cfg["M"], cfg["N"], cfg["sub"]
+    M, N, sub, chunk = cfg["M"], cfg["N"], cfg["sub"], cfg["chunk"]
     g = dict(np.load(GOLDEN_C5))
     checkpoints = sorted(int(k.split("/")[0]) for k in g if k.endswith("/cp"))
     s = Solver(M, N, engine=engine)
     s.set_vertices(v)
     s.set_params(**flow_kwargs(cfg, cfg["cfl"]))
     s.prepare_state("freestream")  # in double for the FP64 engine, as the oracle's
-    out, done = {}, 0
+    out, forces, done = {}, [], 0
     for c in checkpoints:
-        advance(s, c - done, cfg["chunk"])
-        done = c
+        while done < c:
+            n = min(chunk, c - done)
+            s.step(n)
+            done += n
+            f = s.forces()
+            forces.append((f["Cl"], f["Cd"]))
         q = s.state_f64()[1:N + 1]
         rho, p = primitives(q)
-        f = s.forces()
         out[c] = {"rho_sub": rho[::sub, ::sub], "p_sub": p[::sub, ::sub],
-                  "cp": (p[0] - 1.0 / 1.4) / (0.5 * cfg["mach"] ** 2), "Cl": f["Cl"], "Cd": f["Cd"],
+                  "cp": (p[0] - 1.0 / 1.4) / (0.5 * cfg["mach"] ** 2), "Cl": forces[-1][0], "Cd": forces[-1][1],
+                  "chunks": len(forces),
                   "sha": hashlib.sha256(np.ascontiguousarray(q, np.float64).tobytes()).hexdigest(),
                   "finite": bool(np.all(np.isfinite(q)))}
     s.close()
-    C5_ENGINES[engine] = (g, checkpoints, out)
+    C5_ENGINES[engine] = (g, checkpoints, out, np.array(forces))
     return C5_ENGINES[engine]
 
 
@@ -261,9 +266,11 @@ def c5():
 
 def test_config5_subgrid_f64_engine(c5):
     """The full-FP64 GPU engine, which the 4096 x 3072 precision study takes as its FP64
-    solution, against the FP64 oracle on configuration 5's flow at 1024 x 768: density,
-    pressure and wall Cp within 1e-9 of their max at every checkpoint (up to 100000 steps)."""
-    g, checkpoints, out = c5_run(c5, "f64")
+    solution, against the FP64 oracle on configuration 5's flow at 1024 x 768: the whole
+    float64 state bit for bit at every checkpoint (up to 100000 steps; both evaluate the
+    same operations in the same order, correctly rounded, with no contraction), and the
+    sampled fields within 1e-9 of their max as a readable second statement."""
+    g, checkpoints, out, _ = c5_run(c5, "f64")
     for c in checkpoints:
         r = out[c]
         assert r["finite"]
@@ -272,22 +279,35 @@ def test_config5_subgrid_f64_engine(c5):
         print(f"{c} steps: FP64 engine vs FP64 oracle {e} bit-identical state: {same}")
         for name in ("rho_sub", "p_sub", "cp"):
             assert e[name] <= TOL_C5_F64, f"{name} after {c} steps: {e[name]:.3e}"
+        assert same, f"state after {c} steps differs from the FP64 oracle's"
 
 
 def test_config5_subgrid_fp32_error(c5):
     """The FP32 engines' error against the FP64 oracle on configuration 5's flow at
     1024 x 768 (the precision study's comparison at a size the oracle runs on the host
     cores).  The reference-shaped engine is the reference's own float32 arithmetic (bit
-    for bit its shaders), so its error is what any float32 code of this solver incurs on
-    this flow; the fused engine is held to twice that (or 1e-4), field by field and for the
-    lift and drag at every checkpoint."""
-    g, checkpoints, fused = c5_run(c5, "fused")
-    _, _, ref = c5_run(c5, "reference")
+    for bit its shaders), so its error is what a float32 code of this solver incurs on
+    this flow.  At every checkpoint the fused engine's density, pressure and wall Cp
+    (max and L2 over max and norm) are within max(2 x the reference's, 1e-4).  Lift and
+    drag: the M 6 leading-edge region amplifies round-off-sized differences by about 1e5
+    over 20000 steps, after which every float32 run's lift error wanders from one
+    1000-step chunk to the next (1e-5 to 2.4e-3 for the reference's arithmetic from four
+    start states one rounding apart); the fused engine's Cl and Cd are held to twice the
+    largest error the reference-shaped engine showed in any chunk up to that checkpoint
+    (against the FP64 engine, which is the oracle bit for bit), or 1e-4."""
+    g, checkpoints, fused, _ = c5_run(c5, "fused")
+    _, _, ref, ref_forces = c5_run(c5, "reference")
+    _, _, _, f64_forces = c5_run(c5, "f64")
+    ref_force_err = np.abs(ref_forces - f64_forces) / np.abs(f64_forces)  # per chunk: Cl, Cd
     for c in checkpoints:
         assert fused[c]["finite"] and ref[c]["finite"]
         ef, er = c5_errors(fused[c], g, c), c5_errors(ref[c], g, c)
+        envelope = ref_force_err[:ref[c]["chunks"]].max(axis=0)
         print(f"{c} steps vs the FP64 oracle: fused {ef}")
-        print(f"{c} steps vs the FP64 oracle: reference {er}")
-        for name in ef:
+        print(f"{c} steps vs the FP64 oracle: reference {er}; its largest Cl, Cd errors so far {envelope}")
+        for name in ("rho_sub", "rho_sub_l2", "p_sub", "p_sub_l2", "cp", "cp_l2"):
             assert ef[name] <= max(2.0 * er[name], 1e-4), \
                 f"{name} after {c} steps: fused {ef[name]:.3e}, reference's own float32 {er[name]:.3e}"
+        for k, name in enumerate(("Cl", "Cd")):
+            assert ef[name] <= max(2.0 * envelope[k], 1e-4), \
+                f"{name} after {c} steps: fused {ef[name]:.3e}, reference's largest so far {envelope[k]:.3e}"
