@@ -17,7 +17,11 @@ Configuration 1 (NACA 0012, 256 x 128, M 0.5, SLAU2):
     to 1e-4 in Cp at that point; in density they agree to 4.5e-5.
 Configuration 2 (NACA 2412, 512 x 384; M 0.8 SLAU2, M 2 AUSM+-up, M 8 SLAU): one step
   at 1e-5 and 300 steps (frames of 100) at 1e-4 normwise against the float32 oracle run
-  on the host cores in the test.
+  on the host cores in the test; as written (20000 steps) against the float32 oracle's
+  run (tests/golden/baseline_c2.npz).
+Configuration 5 (NACA 0024, M 6, AoA 4, SLAU2) on its 1024 x 768 sub-grid against the
+  FP64 oracle (tests/golden/baseline_c5sub.npz, up to 100000 steps): the full-FP64
+  engine bit for bit, the FP32 engines against the reference's own float32 error.
 """
 import hashlib
 import math
