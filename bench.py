@@ -372,6 +372,62 @@ def run_precision(ausm, steps, chunk=1000, sensitivity=False, reference=False, n
     return out
 
 
+def run_precision_ensemble(ausm, wl, steps, seeds, chunk=1000):
+    """How large a float32 error the flow allows: the fused and the reference-shaped FP32
+    engines (the latter is the reference's arithmetic bit for bit), each from the float32
+    freestream (seed 0) and from seeds - 1 starts with every cell changed by about one
+    float32 rounding (relative N(0, 1e-7), numpy seed k), against the FP64 engine from the
+    freestream in double; dt recomputed every `chunk` steps in all.  Per run: density and
+    pressure errors of the final state (max over max, relative L2), and the lift and drag
+    errors at the end and at the worst chunk; per engine the range over the runs."""
+    import numpy as np
+    g = 1.4
+
+    def run(engine, seed):
+        s = build_solver(ausm, wl)
+        N = s.N
+        if engine == "f64":
+            s.set_engine("f64")
+            s.prepare_state("freestream")  # in double
+        elif engine == "reference":
+            s.set_engine("reference")
+        if seed > 0:
+            q = s.state()
+            rng = np.random.default_rng(seed)
+            q[1:N + 1] *= (1.0 + 1e-7 * rng.standard_normal(q[1:N + 1].shape)).astype(np.float32)
+            s.set_state(q)
+        done, forces = 0, []
+        while done < steps:
+            n = min(chunk, steps - done)
+            s.step(n)
+            done += n
+            f = s.forces()
+            forces.append((f["Cl"], f["Cd"]))
+        q = s.state_f64()[1:N + 1]
+        s.close()
+        rho = q[..., 0]
+        p = (q[..., 3] - 0.5 * (q[..., 1] ** 2 + q[..., 2] ** 2) / rho) * (g - 1.0)
+        return rho, p, np.array(forces)
+
+    r64, p64, f64 = run("f64", 0)
+    out = {"metric": "precision ensemble", "workload": wl["name"], "grid": f"{wl['M']}x{wl['N']}", "steps": steps,
+           "chunk": chunk, "seeds": seeds, "runs": {}, "range": {}}
+    for engine in ("fused", "reference"):
+        for seed in range(seeds):
+            rho, p, f = run(engine, seed)
+            ef = np.abs(f - f64) / np.abs(f64)
+            out["runs"][f"{engine}/{seed}"] = {
+                "rho_max": float(np.abs(rho - r64).max() / np.abs(r64).max()),
+                "rho_l2": float(np.sqrt(np.mean((rho - r64) ** 2)) / np.sqrt(np.mean(r64 ** 2))),
+                "p_max": float(np.abs(p - p64).max() / np.abs(p64).max()),
+                "p_l2": float(np.sqrt(np.mean((p - p64) ** 2)) / np.sqrt(np.mean(p64 ** 2))),
+                "cl_end": float(ef[-1, 0]), "cl_worst_chunk": float(ef[:, 0].max()),
+                "cd_end": float(ef[-1, 1]), "cd_worst_chunk": float(ef[:, 1].max())}
+        runs = [v for k, v in out["runs"].items() if k.startswith(engine + "/")]
+        out["range"][engine] = {key: [min(r[key] for r in runs), max(r[key] for r in runs)] for key in runs[0]}
+    return out
+
+
 def batch_specs(cfg):
     import numpy as np
     rng = np.random.default_rng(cfg["seed"])
@@ -617,6 +673,9 @@ def main():
                     help="also the reference-shaped FP32 engine against FP64")
     ap.add_argument("--precision-sensitivity", action="store_true",
                     help="also an FP64 run from the freestream in double (sensitivity of the flow)")
+    ap.add_argument("--precision-ensemble", type=int, default=0,
+                    help="K > 0: the FP32 engines from K starts one rounding apart against FP64 "
+                         "(on --grid MxN of the same flow, --precision-steps steps)")
     ap.add_argument("--batch-steps", type=int, default=BATCH["steps"],
                     help="steps per solve of the batched measurement (shorter runs for profiling only)")
     ap.add_argument("--no-plain", action="store_true", help="batched measurement without the plain comparison")
@@ -643,6 +702,15 @@ def main():
     ausm.set_device(local_rank % max(1, ausm.device_count()))
     if args.mode == "batch":
         res = run_batched(ausm, dict(BATCH, steps=args.batch_steps), args.warmup, plain=not args.no_plain)
+        if rank == 0:
+            print(json.dumps(res))
+        return 0
+    if args.mode == "precision" and args.precision_ensemble > 0:
+        wl = dict(WORKLOAD)
+        if args.grid:
+            gm, gn = (int(x) for x in args.grid.lower().split("x"))
+            wl.update(M=gm, N=gn, name=f"naca0024_{gm}x{gn}_m6_aoa4_slau2")
+        res = run_precision_ensemble(ausm, wl, args.precision_steps, args.precision_ensemble)
         if rank == 0:
             print(json.dumps(res))
         return 0
