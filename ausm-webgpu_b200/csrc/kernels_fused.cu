@@ -18,7 +18,7 @@
 // on the float bits, as cflReductionShaderCode ausm.js:535-581); the first step's
 // stage 1 turns it into dt.
 //
-// k_fused_tile_tma stages its tile with TMA (cp.async.bulk.tensor, no multicast;
+// k_fused_tile_tma stages its tile with TMA (cp.async.bulk.tensor, each CTA its own boxes;
 // tile_tma.cuh), one tile per CTA, launched with programmatic dependent launch.
 // k_fused_stage loads 32 x 16 tiles with per-thread loads: it evaluates the residual
 // alone (stage 0) and steps a solve whose tensor maps could not be encoded.  Every

@@ -2,7 +2,7 @@
 // (36 x (TY+4) float4), the face-record boxes (33 x TY i-faces, 32 x (TY+1) j-faces),
 // for stages 2 and 3 the Qn box (32 x TY) and, for a tile at the seam, the two columns
 // its halo wraps to (2 x (TY+4)) land in shared memory by cp.async.bulk.tensor copies
-// (no multicast) completing on three mbarriers; the threads then fill the ghost rows
+// (each CTA fetching its own) completing on three mbarriers; the threads then fill the ghost rows
 // the boxes cannot hold and run the tile compute of stage_tile.cuh.  Used by the single-solve kernel (tensor maps as a kernel
 // parameter) and the batched kernel (per-solve tensor maps in global memory, written
 // by the host before the launch).

@@ -1,5 +1,5 @@
 // TMA (cp.async.bulk.tensor) tile loads completed on shared-memory mbarriers, sm_100a.
-// Loads are plain (no cluster multicast).  Every wait is bounded: after kWaitPolls
+// Loads are plain: each CTA fetches its own boxes from this GPU's memory.  Every wait is bounded: after kWaitPolls
 // polls the waiter gives up and the caller reports a timeout instead of hanging.
 #pragma once
 #include <cuda.h>
